@@ -1,0 +1,336 @@
+// C ABI of libemdb200.so (declared in include/emdb200.h): plans, launches,
+// status read-back and error strings.  Host code only; kernels live in
+// emd_sift.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/emdb200.h"
+#include "emdb_internal.cuh"
+
+struct emdb_plan {
+  emdb_config cfg;
+  int device = 0;
+  int num_sms = 0;
+  int smem_optin = 0;
+  int arena_override = 0;
+  int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
+  char* d_slab = nullptr;
+  size_t slab_stride = 0;
+  int slab_ctas = 0;
+  std::mutex mu;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return fail(e == cudaErrorMemoryAllocation ? EMDB_ERR_NOMEM : EMDB_ERR_CUDA, m);
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+// Per-SM shared memory is 228 KB on B200 with 1 KB reserved per CTA; pick the
+// largest arena that still keeps `want` CTAs resident, but never below what a
+// trace of length max_n needs plus a modest knot budget.
+int auto_arena(const emdb_plan* p, int max_n) {
+  const int per_sm = 233472;
+  size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
+  int best = 0;
+  for (int want = 4; want >= 1; --want) {
+    int arena = per_sm / want - 1024;
+    arena = std::min(arena, p->smem_optin);
+    arena &= ~15;
+    // need the fixed part plus room for ~2 x 96 knots before spilling
+    size_t min_need = fixed + (size_t)(11 * 2 * (96 + 2 * p->cfg.nbsym + 2)) * sizeof(double);
+    if ((size_t)arena >= min_need) { best = arena; break; }
+  }
+  if (best == 0) {
+    size_t need = fixed + 64;
+    if (need <= (size_t)p->smem_optin) best = (int)((need + 15) & ~size_t(15));
+  }
+  return best;
+}
+
+int arena_for(const emdb_plan* p, int max_n) {
+  if (p->arena_override > 0) return p->arena_override;
+  return auto_arena(p, max_n);
+}
+
+int ensure_slab(emdb_plan* p, int grid) {
+  if (grid <= p->slab_ctas) return EMDB_OK;
+  if (p->d_slab) cudaFree(p->d_slab);
+  p->d_slab = nullptr;
+  p->slab_ctas = 0;
+  size_t bytes = p->slab_stride * (size_t)grid;
+  cudaError_t e = cudaMalloc(&p->d_slab, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "allocating the spill slab");
+  p->slab_ctas = grid;
+  return EMDB_OK;
+}
+
+int check_config(const emdb_config* c) {
+  if (!c) return fail(EMDB_ERR_INVALID, "config is NULL");
+  if (c->max_extrema < 4 || c->max_extrema > (1 << 20))
+    return fail(EMDB_ERR_INVALID, "max_extrema must be in [4, 2^20]");
+  if (c->nbsym < 1 || c->nbsym > emdb::kMaxNbsym)
+    return fail(EMDB_ERR_INVALID, "nbsym must be in [1, 8]");
+  if (c->max_iteration < 1) return fail(EMDB_ERR_INVALID, "max_iteration must be >= 1");
+  if (c->max_imfs < 2 || c->max_imfs > emdb::kMaxImfsCap)
+    return fail(EMDB_ERR_INVALID, "max_imfs must be in [2, 64]");
+  if (c->threads_per_block != emdb::kThreads)
+    return fail(EMDB_ERR_UNSUPPORTED,
+                "threads_per_block must be 128: the reduction order of the stop tests is defined "
+                "over 128 lanes");
+  return EMDB_OK;
+}
+
+int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st) {
+  int arena = arena_for(p, max_n);
+  if (arena <= 0 || emdb::sift_fixed_smem(max_n) + 64 > (size_t)arena)
+    return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
+                " does not fit this device's shared memory");
+  int per_sm = 0;
+  cudaError_t e = emdb::sift_occupancy(arena, &per_sm);
+  if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
+  int grid = std::min(sp.batch, per_sm * p->num_sms);
+  int rc = ensure_slab(p, grid);
+  if (rc) return rc;
+  sp.queue = p->d_ctl;
+  sp.status = p->d_ctl + 1;
+  sp.slab = p->d_slab;
+  sp.slab_stride = p->slab_stride;
+  sp.arena_bytes = arena;
+  sp.max_extrema = p->cfg.max_extrema;
+  sp.nbsym = p->cfg.nbsym;
+  sp.max_iteration = p->cfg.max_iteration;
+  sp.max_imfs = p->cfg.max_imfs;
+  e = cudaMemsetAsync(p->d_ctl, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "queue reset");
+  e = emdb::launch_sift(sp, grid, st);
+  if (e != cudaSuccess) return cuda_fail(e, "sift launch");
+  return EMDB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int emdb_version(void) { return 10000; }
+
+int emdb_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    std::strncpy(buf, g_last_error.c_str(), len - 1);
+    buf[len - 1] = 0;
+  }
+  return EMDB_OK;
+}
+
+int emdb_plan_create(const emdb_config* cfg, int device, emdb_plan** out) {
+  if (!out) return fail(EMDB_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+  if (device < 0 || device >= ndev) return fail(EMDB_ERR_INVALID, "device out of range");
+  DeviceGuard g(device);
+  emdb_plan* p = new emdb_plan();
+  p->cfg = *cfg;
+  p->device = device;
+  cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&p->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  p->slab_stride = emdb::sift_slab_bytes(cfg->max_extrema, cfg->nbsym);
+  e = cudaMalloc(&p->d_ctl, 4 * sizeof(int));
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_fail(e, "allocating plan control words");
+  }
+  cudaMemset(p->d_ctl, 0, 4 * sizeof(int));
+  *out = p;
+  return EMDB_OK;
+}
+
+int emdb_plan_destroy(emdb_plan* p) {
+  if (!p) return EMDB_OK;
+  {
+    DeviceGuard g(p->device);
+    if (p->d_slab) cudaFree(p->d_slab);
+    if (p->d_ctl) cudaFree(p->d_ctl);
+  }
+  delete p;
+  return EMDB_OK;
+}
+
+int emdb_plan_set_arena(emdb_plan* p, int arena_bytes) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (arena_bytes < 0 || arena_bytes > p->smem_optin)
+    return fail(EMDB_ERR_INVALID, "arena exceeds the device's per-block shared memory");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->arena_override = arena_bytes & ~15;
+  return EMDB_OK;
+}
+
+int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm, int* grid_max) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  DeviceGuard g(p->device);
+  int arena = arena_for(p, max_n);
+  int per_sm = 0;
+  if (arena > 0) {
+    cudaError_t e = emdb::sift_occupancy(arena, &per_sm);
+    if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  }
+  if (arena_bytes) *arena_bytes = arena;
+  if (ctas_per_sm) *ctas_per_sm = per_sm;
+  if (grid_max) *grid_max = per_sm * p->num_sms;
+  return EMDB_OK;
+}
+
+int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, int N,
+             double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
+             void* stream) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
+  if (batch == 0) return EMDB_OK;
+  if ((N > 0 && (!signals || !imfs)) || !n_imfs || !overflow || !dbg_n || !dbg_extno || !dbg_nzm)
+    return fail(EMDB_ERR_INVALID, "NULL buffer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  emdb::SiftParams sp{};
+  sp.values = signals;
+  sp.offsets = nullptr;
+  sp.dense_n = N;
+  sp.T = T;
+  sp.t_mode = T ? emdb::kTShared : emdb::kTArange;
+  sp.batch = batch;
+  sp.order = nullptr;
+  sp.imfs = imfs;
+  sp.n_imfs = n_imfs;
+  sp.overflow = overflow;
+  sp.dbg_n = dbg_n;
+  sp.dbg_ext = dbg_extno;
+  sp.dbg_nzm = dbg_nzm;
+  return launch_common(p, sp, N, (cudaStream_t)stream);
+}
+
+int emdb_run_ragged(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
+                    int max_n, const double* T, int t_per_trace, const int* order, double* imfs,
+                    int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
+                    void* stream) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (batch < 0 || max_n < 0) return fail(EMDB_ERR_INVALID, "batch and max_n must be >= 0");
+  if (batch == 0) return EMDB_OK;
+  if (!values || !offsets || !imfs || !n_imfs || !overflow || !dbg_n || !dbg_extno || !dbg_nzm)
+    return fail(EMDB_ERR_INVALID, "NULL buffer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  emdb::SiftParams sp{};
+  sp.values = values;
+  sp.offsets = offsets;
+  sp.dense_n = 0;
+  sp.T = T;
+  sp.t_mode = T ? (t_per_trace ? emdb::kTPerTrace : emdb::kTShared) : emdb::kTArange;
+  sp.batch = batch;
+  sp.order = order;
+  sp.imfs = imfs;
+  sp.n_imfs = n_imfs;
+  sp.overflow = overflow;
+  sp.dbg_n = dbg_n;
+  sp.dbg_ext = dbg_extno;
+  sp.dbg_nzm = dbg_nzm;
+  return launch_common(p, sp, max_n, (cudaStream_t)stream);
+}
+
+int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batch, int N,
+                  double* max_env, double* min_env, int* n_extrema, int* degenerate,
+                  double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
+                  int* n_mirrored, void* stream) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
+  if (batch == 0) return EMDB_OK;
+  if (!signals || !max_env || !min_env || !n_extrema || !degenerate || !max_kpos || !max_kval ||
+      !min_kpos || !min_kval || !n_mirrored)
+    return fail(EMDB_ERR_INVALID, "NULL buffer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int arena = arena_for(p, N);
+  if (arena <= 0 || emdb::sift_fixed_smem(N) + 64 > (size_t)arena)
+    return fail(EMDB_ERR_UNSUPPORTED, "trace length does not fit this device's shared memory");
+  int per_sm = 0;
+  cudaError_t e = emdb::envelope_occupancy(arena, &per_sm);
+  if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+  if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
+  int grid = std::min(batch, per_sm * p->num_sms);
+  int rc = ensure_slab(p, grid);
+  if (rc) return rc;
+  emdb::EnvParams ep{};
+  ep.values = signals;
+  ep.offsets = nullptr;
+  ep.dense_n = N;
+  ep.T = T;
+  ep.t_mode = T ? emdb::kTShared : emdb::kTArange;
+  ep.batch = batch;
+  ep.max_env = max_env;
+  ep.min_env = min_env;
+  ep.n_extrema = n_extrema;
+  ep.degenerate = degenerate;
+  ep.max_kpos = max_kpos;
+  ep.max_kval = max_kval;
+  ep.min_kpos = min_kpos;
+  ep.min_kval = min_kval;
+  ep.n_mirrored = n_mirrored;
+  ep.mbuf = p->cfg.max_extrema + 2 * p->cfg.nbsym;
+  ep.queue = p->d_ctl + 2;
+  ep.status = p->d_ctl + 1;
+  ep.slab = p->d_slab;
+  ep.slab_stride = p->slab_stride;
+  ep.arena_bytes = arena;
+  ep.max_extrema = p->cfg.max_extrema;
+  ep.nbsym = p->cfg.nbsym;
+  e = cudaMemsetAsync(p->d_ctl + 2, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "queue reset");
+  e = emdb::launch_envelope(ep, grid, st);
+  if (e != cudaSuccess) return cuda_fail(e, "envelope launch");
+  return EMDB_OK;
+}
+
+int emdb_status(emdb_plan* p, int* status, void* stream) {
+  if (!p || !status) return fail(EMDB_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, p->d_ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->d_ctl + 1, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "status read-back");
+  *status = v;
+  return EMDB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Internal declarations shared by the sift kernels and the C-ABI host code.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+namespace emdb {
+
+constexpr int kThreads = 128;   // one CTA = 128 threads = the reference's 128 reduction lanes
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxNbsym = 8;
+constexpr int kMaxImfsCap = 64;
+
+// Status bits a kernel may raise (device-side error word, never a trap).
+enum : int {
+  kStatusStaleEnvelope = 1,   // a sample fell outside the knot span (needs non-monotone T)
+  kStatusTooLong = 2,         // a trace does not fit the launch's shared-memory arena
+};
+
+// Time axis modes.
+enum : int { kTArange = 0, kTShared = 1, kTPerTrace = 2 };
+
+struct SiftParams {
+  // input: CSR traces (dense [B,N] is offsets b*N)
+  const double* values;
+  const int64_t* offsets;     // [batch+1], or NULL for a dense [batch, dense_n] batch
+  int dense_n;
+  const double* T;            // per t_mode
+  int t_mode;
+  int batch;
+  const int* order;           // queue order (NULL = FIFO)
+  // outputs: trace b's rows start at imfs + max_imfs*offsets[b], row r at +r*N_b
+  double* imfs;
+  int* n_imfs;
+  int* overflow;
+  int* dbg_n;
+  int* dbg_ext;
+  int* dbg_nzm;
+  // scratch
+  int* queue;                 // work-queue ticket counter (zeroed before launch)
+  int* status;                // error word (OR of kStatus*)
+  char* slab;                 // per-CTA global spill area
+  size_t slab_stride;         // bytes per CTA
+  int arena_bytes;            // dynamic shared memory per CTA
+  // config (EMDKernelConfig fields)
+  int max_extrema;
+  int nbsym;
+  int max_iteration;
+  int max_imfs;
+};
+
+struct EnvParams {
+  const double* values;
+  const int64_t* offsets;     // NULL = dense [batch, dense_n]
+  int dense_n;
+  const double* T;
+  int t_mode;
+  int batch;
+  double* max_env;            // CSR like values
+  double* min_env;
+  int* n_extrema;             // [batch,2]
+  int* degenerate;            // [batch]
+  double* max_kpos;           // [batch, mbuf]
+  double* max_kval;
+  double* min_kpos;
+  double* min_kval;
+  int* n_mirrored;            // [batch,2]
+  int mbuf;
+  int* queue;
+  int* status;
+  char* slab;
+  size_t slab_stride;
+  int arena_bytes;
+  int max_extrema;
+  int nbsym;
+};
+
+// Shared-memory bytes a CTA needs beyond the knot arena for a trace of length N.
+size_t sift_fixed_smem(int N);
+// Worst-case global spill bytes per CTA for a given extrema cap / nbsym.
+size_t sift_slab_bytes(int max_extrema, int nbsym);
+
+cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream);
+cudaError_t sift_occupancy(int arena_bytes, int* ctas_per_sm);
+cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm);
+
+}  // namespace emdb

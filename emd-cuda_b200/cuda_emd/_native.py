@@ -1,0 +1,129 @@
+"""ctypes binding of libemdb200.so (C ABI in include/emdb200.h).
+
+There is no fallback: if the library is missing or no CUDA device is present,
+using the binding raises.  Build the library with
+``python emd-cuda_b200/build.py``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libemdb200.so")
+
+EMDB_OK = 0
+EMDB_ERR_INVALID = 1
+EMDB_ERR_CUDA = 2
+EMDB_ERR_NOMEM = 3
+EMDB_ERR_UNSUPPORTED = 4
+EMDB_ERR_DEVICE = 5
+STATUS_STALE_ENVELOPE = 1
+STATUS_TOO_LONG = 2
+
+# Every symbol include/emdb200.h declares (checked by the CPU test suite).
+EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_set_arena",
+           "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
+           "emdb_last_error")
+
+
+class EmdbConfig(ctypes.Structure):
+    _fields_ = [("max_extrema", ctypes.c_int), ("nbsym", ctypes.c_int),
+                ("max_iteration", ctypes.c_int), ("max_imfs", ctypes.c_int),
+                ("threads_per_block", ctypes.c_int)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib_path() -> str:
+    return LIB_PATH
+
+
+def load() -> ctypes.CDLL:
+    """Load the library (once).  Raises OSError if it is not built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.isfile(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is not built; run `python emd-cuda_b200/build.py`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, VP = ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p
+        L.emdb_version.restype = I
+        L.emdb_plan_create.argtypes = [ctypes.POINTER(EmdbConfig), I, ctypes.POINTER(VP)]
+        L.emdb_plan_destroy.argtypes = [VP]
+        L.emdb_plan_set_arena.argtypes = [VP, I]
+        L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
+        L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
+        L.emdb_run_ragged.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]
+        L.emdb_envelope.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
+        L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
+        L.emdb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        for name in EXPORTS:
+            getattr(L, name).restype = I
+        _lib = L
+        return L
+
+
+def last_error() -> str:
+    L = load()
+    buf = ctypes.create_string_buffer(1024)
+    L.emdb_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+class EmdbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def check(rc: int, what: str) -> None:
+    """Map a C-ABI return code to the reference's exception types."""
+    if rc == EMDB_OK:
+        return
+    msg = f"{what}: {last_error()}"
+    if rc in (EMDB_ERR_INVALID, EMDB_ERR_UNSUPPORTED):
+        raise ValueError(msg)
+    if rc == EMDB_ERR_NOMEM:
+        raise MemoryError(msg)
+    raise EmdbError(rc, msg)
+
+
+class Plan:
+    """Owns one emdb_plan (device scratch + config) for one CUDA device."""
+
+    def __init__(self, cfg: EmdbConfig, device: int):
+        self.L = load()
+        self.device = device
+        h = ctypes.c_void_p()
+        check(self.L.emdb_plan_create(ctypes.byref(cfg), device, ctypes.byref(h)), "emdb_plan_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.L.emdb_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_arena(self, arena_bytes: int) -> None:
+        check(self.L.emdb_plan_set_arena(self.handle, int(arena_bytes)), "emdb_plan_set_arena")
+
+    def query(self, max_n: int) -> tuple[int, int, int]:
+        a, c, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self.L.emdb_plan_query(self.handle, int(max_n), ctypes.byref(a), ctypes.byref(c),
+                                     ctypes.byref(g)), "emdb_plan_query")
+        return a.value, c.value, g.value
+
+    def status(self, stream: int) -> int:
+        s = ctypes.c_int()
+        check(self.L.emdb_status(self.handle, ctypes.byref(s), ctypes.c_void_p(stream)), "emdb_status")
+        return s.value

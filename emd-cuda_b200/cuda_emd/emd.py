@@ -1,0 +1,123 @@
+"""GPUBatchEMD -- drop-in for the reference's host wrapper
+(SeismicFlow/emd-cuda emd.py:53-114) over the B200 kernels.
+
+    from cuda_emd.emd import GPUBatchEMD
+    gpu_emd = GPUBatchEMD()
+    gpu_emd.warmup()
+    imfs, n_imfs, overflow = gpu_emd(signals)      # signals [batch, N] float64
+
+``imfs`` is [batch, MAX_IMFS, N] float64, ``n_imfs`` / ``overflow`` [batch]
+int32, ``last_debug`` holds (debug_n, debug_extno, debug_nzm) [batch, MAX_IMFS].
+Results are returned in the caller's array framework (torch, CuPy or NumPy).
+
+Beyond the reference: ``ragged(values, offsets, order=None)`` decomposes a
+CSR batch of mixed-length traces in one launch.
+"""
+from __future__ import annotations
+
+import warnings
+
+import numpy as np
+
+try:
+    from .kernels import EMDKernelConfig
+except ImportError:  # flat layout: emd.py and kernels.py side by side
+    from kernels import EMDKernelConfig  # type: ignore
+
+
+def _normalise_T(T, N: int, device: int):
+    """emd.py:83-88: arange(N) if T is None, else (T - T[0]) / min(diff(T)).
+    None stays None (the kernel then uses arange without a buffer).  The
+    normalised axis must be finite and strictly increasing; the reference
+    would read stale envelope values otherwise, so this build refuses it."""
+    if T is None:
+        return None
+    import torch
+    from ._arrays import as_device_f64
+    Td, _ = as_device_f64(T, device)
+    if Td.dim() != 1 or Td.shape[0] != N:
+        raise ValueError(f"T must be 1-D of length {N}")
+    if N < 2:
+        return Td - Td[0] if N == 1 else Td
+    d = Td[1:] - Td[:-1]
+    Tn = (Td - Td[0]) / torch.min(d)
+    dn = Tn[1:] - Tn[:-1]
+    if not bool(torch.isfinite(Tn).all()) or not bool((dn > 0).all()):
+        raise ValueError("T must normalise to a finite, strictly increasing axis")
+    return Tn
+
+
+class GPUBatchEMD:
+    def __init__(self, config: "EMDKernelConfig | None" = None):
+        self._config = config or EMDKernelConfig.for_device()
+        self._launcher = None
+        self.last_debug = None
+
+    @property
+    def config(self) -> EMDKernelConfig:
+        return self._config
+
+    def warmup(self, N: int = 64) -> None:
+        """One tiny real call (an all-zero trace, emd.py:58-64) so that plan
+        creation and first-launch costs land here, not in a timed call."""
+        import torch
+        self(torch.zeros((1, N), dtype=torch.float64, device="cuda"))
+
+    def _get_launcher(self):
+        if self._launcher is None:
+            self._launcher = self._config.build()
+        return self._launcher
+
+    def _overflow_warning(self, overflow, batch: int) -> None:
+        import torch
+        ov = overflow if isinstance(overflow, torch.Tensor) else torch.as_tensor(np.asarray(overflow))
+        n_hit = int(ov.sum().item())
+        if n_hit:
+            warnings.warn(
+                f"{n_hit}/{batch} signal(s) hit MAX_EXTREMA or MAX_ITERATION during "
+                "sifting -- their output is not a verified decomposition. Check the "
+                "`overflow` array to find which, and raise EMDKernelConfig.max_extrema "
+                "/ max_iteration for those.",
+                stacklevel=3,
+            )
+
+    def __call__(self, signals, T=None):
+        if signals.ndim == 1:
+            signals = signals[None, :]
+        dt = np.dtype(str(signals.dtype).replace("torch.", ""))
+        if dt != np.dtype(np.float64):
+            raise ValueError(
+                f"GPUBatchEMD (this build) is float64 only, got {signals.dtype}. "
+                f"Cast explicitly first, e.g. signals.astype(float64) -- this "
+                f"class won't silently do that for you."
+            )
+        launcher = self._get_launcher()
+        batch, N = signals.shape
+        Tn = _normalise_T(T, N, launcher.device)
+        imfs, n_imfs, overflow, dn, de, dz = launcher.run(signals, Tn)
+        self.last_debug = (dn, de, dz)
+        launcher.check_status()
+        self._overflow_warning(overflow, batch)
+        return imfs, n_imfs, overflow
+
+    def ragged(self, values, offsets, order=None, max_n: int | None = None):
+        """Decompose a CSR batch (values f64 [total], offsets int64 [batch+1]) in
+        one launch, T = arange(N_b) per trace.  ``order`` (int32 permutation) only
+        sets the queue order.  Returns (imfs_csr, n_imfs, overflow)."""
+        launcher = self._get_launcher()
+        imfs, n_imfs, overflow, dn, de, dz = launcher.run_ragged(values, offsets, order=order,
+                                                                 max_n=max_n)
+        self.last_debug = (dn, de, dz)
+        launcher.check_status()
+        self._overflow_warning(overflow, n_imfs.shape[0])
+        return imfs, n_imfs, overflow
+
+    def unpack(self, imfs, n_imfs, i: int):
+        """Signal i's rows [n_imfs[i], N] as a NumPy array (emd.py:109-114)."""
+        k = int(n_imfs[i].item() if hasattr(n_imfs[i], "item") else n_imfs[i])
+        x = imfs[i, :k, :]
+        if hasattr(x, "cpu"):
+            return x.cpu().numpy()
+        if hasattr(x, "get"):
+            return x.get()
+        return np.asarray(x)

@@ -1,0 +1,116 @@
+/*
+ * emdb200.h -- C ABI of the B200-native batched EMD (libemdb200.so).
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA device memory on
+ * the plan's device; `stream` is a cudaStream_t passed as void* (NULL = the
+ * legacy default stream).  Every function returns EMDB_OK (0) or an error
+ * code; emdb_last_error() gives the message for the calling thread.  Calls
+ * are asynchronous on `stream` unless stated.  One plan owns scratch (work
+ * queue ticket, status word, per-CTA spill slab); calls on the same plan are
+ * serialised by the plan, calls on distinct plans are independent.
+ *
+ * Reference interface each entry point replaces (SeismicFlow/emd-cuda):
+ *   emdb_plan_create   EMDKernelConfig.build() + EMDBatchLauncher.__init__
+ *                      (kernels.py:1277-1286, 1294-1341): config check,
+ *                      shared-memory opt-in, occupancy sizing
+ *   emdb_run           EMDBatchLauncher.run (kernels.py:1343-1372) launching
+ *                      emd_batch_kernel (kernels.py:834-1080)
+ *   emdb_run_ragged    no reference counterpart for mixed lengths: the
+ *                      reference only takes [batch, N]; this is run() over
+ *                      CSR traces with an optional queue order
+ *   emdb_envelope      EMDBatchLauncher.run_envelope_only (kernels.py:1374-1407)
+ *                      launching envelope_batch_kernel (kernels.py:1100-1166)
+ *   emdb_status        the overflow / error read-back GPUBatchEMD.__call__
+ *                      does after the launch (emd.py:95-105)
+ */
+#ifndef EMDB200_H
+#define EMDB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EMDB_OK 0
+#define EMDB_ERR_INVALID 1      /* bad argument (maps to ValueError) */
+#define EMDB_ERR_CUDA 2         /* CUDA runtime error (RuntimeError) */
+#define EMDB_ERR_NOMEM 3        /* device allocation failed (MemoryError) */
+#define EMDB_ERR_UNSUPPORTED 4  /* config does not fit this device (ValueError) */
+#define EMDB_ERR_DEVICE 5       /* kernel raised a status bit (RuntimeError) */
+
+/* Device status bits returned by emdb_status. */
+#define EMDB_STATUS_STALE_ENVELOPE 1 /* a sample fell outside the knot span */
+#define EMDB_STATUS_TOO_LONG 2       /* a trace did not fit the shared-memory arena */
+
+/* Field-for-field the reference's EMDKernelConfig (kernels.py:1170-1176). */
+typedef struct emdb_config {
+  int max_extrema;       /* per-side extrema cap; >= cap sets overflow (default 1024) */
+  int nbsym;             /* mirrored boundary points per side, 1..8 (default 2) */
+  int max_iteration;     /* sift cap per IMF; reaching it sets overflow (default 1000) */
+  int max_imfs;          /* output rows per trace, 2..64 (default 16) */
+  int threads_per_block; /* reference block size; only 128 is accepted (reduction order) */
+} emdb_config;
+
+typedef struct emdb_plan emdb_plan;
+
+int emdb_version(void);
+
+/* Create a plan for `device`.  Validates the config, opts the kernels into
+ * dynamic shared memory and allocates the plan's scratch. */
+int emdb_plan_create(const emdb_config* cfg, int device, emdb_plan** out);
+int emdb_plan_destroy(emdb_plan* plan);
+
+/* Shared-memory arena per CTA for the next launches (0 = automatic).  The
+ * autotuner sets this; larger arenas spill fewer knots but fit fewer CTAs
+ * per SM.  Fails if the arena cannot hold a trace of length max_n. */
+int emdb_plan_set_arena(emdb_plan* plan, int arena_bytes);
+/* Arena and CTAs/SM the plan would use for traces up to max_n. */
+int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
+                    int* grid_max);
+
+/* Dense batch, the reference's run(): signals [batch, N], T [N] or NULL
+ * (= arange(N), already normalised as emd.py:83-88 does), outputs
+ * imfs [batch, max_imfs, N], n_imfs [batch], overflow [batch],
+ * dbg_n / dbg_extno / dbg_nzm [batch, max_imfs] (-1 = slot not reached).
+ * Every output element is written (no pre-zeroing needed). */
+int emdb_run(emdb_plan* plan, const double* signals, const double* T, int batch, int N,
+             double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+             int* dbg_nzm, void* stream);
+
+/* CSR batch of mixed lengths in one launch: trace b is
+ * values[offsets[b] .. offsets[b+1]), offsets is a DEVICE int64 [batch+1]
+ * array, max_n = max trace length (host value, sizes the arena).
+ * T: NULL = arange per trace; else CSR-aligned per-trace time axes
+ * (t_per_trace = 1) or one shared axis of length max_n (t_per_trace = 0).
+ * order: DEVICE int32 [batch] permutation giving the queue order, or NULL
+ * for FIFO; it changes only which CTA runs a trace when, never a result.
+ * Outputs: trace b's rows at imfs + max_imfs*offsets[b], row r at +r*N_b. */
+int emdb_run_ragged(emdb_plan* plan, const double* values, const int64_t* offsets, int batch,
+                    int max_n, const double* T, int t_per_trace, const int* order,
+                    double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                    int* dbg_nzm, void* stream);
+
+/* Extrema + mirroring + both envelopes on raw traces, no sift loop
+ * (run_envelope_only): max_env/min_env [batch, N], n_extrema [batch, 2],
+ * degenerate [batch], knot positions/values [batch, mbuf] each with
+ * mbuf = max_extrema + 2*nbsym, n_mirrored [batch, 2].  Knot slots past
+ * n_mirrored and envelopes of degenerate traces are written as zero. */
+int emdb_envelope(emdb_plan* plan, const double* signals, const double* T, int batch, int N,
+                  double* max_env, double* min_env, int* n_extrema, int* degenerate,
+                  double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
+                  int* n_mirrored, void* stream);
+
+/* Synchronise `stream`, read and clear the plan's device status word
+ * (EMDB_STATUS_* bits) into *status. */
+int emdb_status(emdb_plan* plan, int* status, void* stream);
+
+/* Message of the calling thread's last error ("" if none). */
+int emdb_last_error(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMDB200_H */

@@ -1,0 +1,180 @@
+"""GPU parity: the B200 kernels (through the C ABI) against the reference's
+own kernel outputs (golden fixtures), the CPU oracle, and -- when
+``oracle/_ref`` is built -- the reference kernel run live on the same GPU.
+
+Bar: bit-identical IMFs (SHA-256 of each trace's [MAX_IMFS, N] block) and
+identical discrete outputs against the ``-fmad=false`` reference build and
+the oracle; against the stock reference build (FMA contraction on) identical
+discrete outputs and IMF values within 1e-9 x signal range.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+IMF_RTOL = 1e-9
+
+
+def _sha(block):
+    return hashlib.sha256(np.ascontiguousarray(block, dtype="<f8").tobytes()).hexdigest().encode()
+
+
+def _cfg(c):
+    from cuda_emd import EMDKernelConfig
+    return EMDKernelConfig(max_extrema=int(c[0]), nbsym=int(c[1]), max_iteration=int(c[2]),
+                           max_imfs=int(c[3]), threads_per_block=int(c[4]))
+
+
+def _run_np(cfg, X, T):
+    import torch
+    L = cfg.build()
+    sig = torch.from_numpy(np.ascontiguousarray(X)).cuda()
+    Td = torch.from_numpy(np.ascontiguousarray(T)).cuda()
+    out = L.run(sig, Td)
+    L.check_status()
+    return [o.cpu().numpy() for o in out]
+
+
+@pytest.mark.parametrize("name", [g["name"] for g in cases.groups()])
+def test_golden_bitexact(golden, name):
+    X = golden[f"{name}__signals"]
+    T = golden[f"{name}__T"]
+    imfs, n_imfs, ovf, dn, de, dz = _run_np(_cfg(golden[f"{name}__cfg"]), X, T)
+    for b in range(X.shape[0]):
+        assert n_imfs[b] == golden[f"{name}__nofma__n_imfs"][b], (name, b)
+        assert ovf[b] == golden[f"{name}__nofma__overflow"][b], (name, b)
+        np.testing.assert_array_equal(dn[b], golden[f"{name}__nofma__dbg_n"][b])
+        np.testing.assert_array_equal(de[b], golden[f"{name}__nofma__dbg_ext"][b])
+        np.testing.assert_array_equal(dz[b], golden[f"{name}__nofma__dbg_nzm"][b])
+        assert _sha(imfs[b]) == golden[f"{name}__nofma__sha"][b], (name, b)
+        # the stock (FMA) reference build: same discrete outputs
+        assert n_imfs[b] == golden[f"{name}__stock__n_imfs"][b]
+        np.testing.assert_array_equal(dn[b], golden[f"{name}__stock__dbg_n"][b])
+
+
+def test_golden_values_vs_stock(golden):
+    for name in ("edge512", "cfg0", "cfg1", "tiny6", "nonuniformT"):
+        X = golden[f"{name}__signals"]
+        T = golden[f"{name}__T"]
+        imfs = _run_np(_cfg(golden[f"{name}__cfg"]), X, T)[0]
+        sel = list(golden[f"{name}__stock__sel"])
+        rows = golden[f"{name}__stock__rows"]
+        flat = golden[f"{name}__stock__imfs"]
+        off = np.concatenate([[0], np.cumsum(rows)])
+        for j, b in enumerate(sel):
+            ref = flat[off[j]:off[j + 1]]
+            rng = float(np.ptp(X[b])) or 1.0
+            assert np.max(np.abs(imfs[b, :ref.shape[0]] - ref)) <= IMF_RTOL * rng
+
+
+def test_envelope_only_golden(golden):
+    import torch
+    from cuda_emd import EMDKernelConfig
+    name = cases.ENVELOPE_GROUP
+    X = golden[f"{name}__signals"]
+    T = golden[f"{name}__T"]
+    L = EMDKernelConfig().build()
+    out = [o.cpu().numpy() for o in L.run_envelope_only(torch.from_numpy(X).cuda(),
+                                                         torch.from_numpy(T).cuda())]
+    emax, emin, next_, deg, kp0, kv0, kp1, kv1, nmir = out
+    np.testing.assert_array_equal(next_, golden[f"{name}__env__n_extrema"])
+    np.testing.assert_array_equal(deg, golden[f"{name}__env__degenerate"])
+    np.testing.assert_array_equal(nmir, golden[f"{name}__env__n_mirrored"])
+    np.testing.assert_array_equal(kp0, golden[f"{name}__env__max_kpos"])
+    np.testing.assert_array_equal(kv0, golden[f"{name}__env__max_kval"])
+    np.testing.assert_array_equal(kp1, golden[f"{name}__env__min_kpos"])
+    np.testing.assert_array_equal(kv1, golden[f"{name}__env__min_kval"])
+    for b in range(X.shape[0]):
+        rng = float(np.ptp(X[b])) or 1.0
+        assert np.max(np.abs(emax[b] - golden[f"{name}__env__max_env"][b])) <= IMF_RTOL * rng
+        assert np.max(np.abs(emin[b] - golden[f"{name}__env__min_env"][b])) <= IMF_RTOL * rng
+
+
+def test_oracle_fresh_inputs():
+    """Fresh seeded inputs (not in the fixtures) against the oracle, bit for bit."""
+    from cuda_emd import EMDKernelConfig, workloads as W
+    from oracle import emd_oracle as O
+    for X in (W.sinusoid_batch(12, 1024, seed=100), W.seismic_batch(4, 2048, seed=101)):
+        T = np.arange(X.shape[1], dtype=np.float64)
+        imfs, n_imfs, ovf, dn, de, dz = _run_np(EMDKernelConfig(), X, T)
+        for b in range(X.shape[0]):
+            r = O.emd_signal(X[b], T)
+            assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
+            np.testing.assert_array_equal(dn[b], r.debug_n)
+            np.testing.assert_array_equal(de[b], r.debug_extno)
+            np.testing.assert_array_equal(dz[b], r.debug_nzm)
+            assert _sha(imfs[b]) == _sha(r.imfs)
+
+
+def test_ragged_matches_oracle_and_order():
+    """CSR batch of mixed lengths in one launch: every trace equals the oracle
+    bit for bit, and a permuted queue order changes nothing."""
+    import torch
+    from cuda_emd import EMDKernelConfig, workloads as W
+    from oracle import emd_oracle as O
+    vals, offs, kinds = W.ragged_mix(24, lo=64, hi=2048, seed=5)
+    L = EMDKernelConfig().build()
+    v = torch.from_numpy(vals).cuda()
+    o = torch.from_numpy(offs).cuda()
+    a = [x.cpu().numpy() for x in L.run_ragged(v, o)]
+    L.check_status()
+    perm = torch.from_numpy(np.random.default_rng(0).permutation(24).astype(np.int32)).cuda()
+    b_ = [x.cpu().numpy() for x in L.run_ragged(v, o, order=perm)]
+    for x, y in zip(a, b_):
+        np.testing.assert_array_equal(x, y)
+    imfs, n_imfs, ovf, dn, de, dz = a
+    mi = 16
+    for b in range(24):
+        N = int(offs[b + 1] - offs[b])
+        r = O.emd_signal(vals[offs[b]:offs[b + 1]], np.arange(N, dtype=np.float64))
+        blk = imfs[mi * offs[b]: mi * offs[b + 1]].reshape(mi, N)
+        assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
+        np.testing.assert_array_equal(dn[b], r.debug_n)
+        assert _sha(blk) == _sha(r.imfs), b
+
+
+def test_api_errors_and_overflow_warning():
+    import torch
+    from cuda_emd import GPUBatchEMD, EMDKernelConfig
+    emd = GPUBatchEMD()
+    with pytest.raises(ValueError):
+        emd(torch.zeros((2, 64), dtype=torch.float32, device="cuda"))
+    emd_small = GPUBatchEMD(EMDKernelConfig(max_extrema=128, max_iteration=6))
+    x = torch.from_numpy(np.random.default_rng(3).normal(size=(2, 512))).cuda()
+    with pytest.warns(UserWarning):
+        imfs, n_imfs, ovf = emd_small(x)
+    assert int(ovf.sum()) == 2
+    emd.warmup()
+    imfs, n_imfs, ovf = emd(x)
+    k = emd.unpack(imfs, n_imfs, 0)
+    assert k.shape == (int(n_imfs[0]), 512)
+    # NumPy in -> NumPy out; 1-D input is promoted
+    out = emd(np.sin(np.arange(256) * 0.3))
+    assert isinstance(out[0], np.ndarray) and out[0].shape == (1, 16, 256)
+
+
+@pytest.mark.skipif(not __import__("refkernel").have_ref(), reason="oracle/_ref not built")
+def test_live_reference_kernel_cfg1_subsample():
+    """cfg1-type traces (2048 samples) through the reference's own kernel on the
+    same GPU: bit-identical to its -fmad=false build, discrete-identical and
+    within tolerance of its stock build."""
+    import torch
+    from refkernel import RefKernel
+    from cuda_emd import EMDKernelConfig, workloads as W
+    X = W.seismic_batch(256, 2048, seed=77)
+    T = np.arange(2048, dtype=np.float64)
+    mine = _run_np(EMDKernelConfig(), X, T)
+    nofma = RefKernel("libemd_ref_nofma.so").run(X, T)
+    stock = RefKernel("libemd_ref.so").run(X, T)
+    for k in range(1, 6):
+        np.testing.assert_array_equal(mine[k], nofma[k])
+    np.testing.assert_array_equal(mine[0], nofma[0])
+    for k in range(1, 6):
+        np.testing.assert_array_equal(mine[k], stock[k])
+    rng = np.ptp(X, axis=1)
+    err = np.abs(mine[0] - stock[0]).max(axis=(1, 2))
+    assert np.all(err <= IMF_RTOL * rng)
