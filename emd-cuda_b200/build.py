@@ -25,9 +25,10 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH, f"-I{I
 # (source, extra flags)
 UNITS = [
     ("emd_sift.cu", ["-fmad=false"]),
+    ("emd_sched.cu", []),
     ("emdb_api.cu", []),
 ]
-HEADERS = ["emdb_internal.cuh"]
+HEADERS = ["emdb_internal.cuh", "emdb_sched.cuh"]
 
 
 def _nvcc() -> str:

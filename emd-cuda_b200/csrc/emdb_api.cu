@@ -334,3 +334,84 @@ int emdb_status(emdb_plan* p, int* status, void* stream) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Cost-model entry points (kernels in emd_sched.cu).
+// ---------------------------------------------------------------------------
+#include "emdb_sched.cuh"
+
+extern "C" {
+
+int emdb_features(const double* values, const int64_t* offsets, int batch, int N, float* feat,
+                  void* stream) {
+  if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
+  if (batch == 0) return EMDB_OK;
+  if (!values || !feat) return fail(EMDB_ERR_INVALID, "NULL buffer");
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  emdb::FeatParams p{values, offsets, N, batch, feat};
+  cudaError_t e = emdb::launch_features(p, std::min(batch, sms * 8), (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "features launch");
+  return EMDB_OK;
+}
+
+int emdb_mlp_num_params(void) { return emdb::kNParams; }
+
+int emdb_mlp_forward(const float* params, const float* X, const float* mu, const float* sd, int B,
+                     float* Z1, float* H1, float* Z2, float* H2, float* Y, void* stream) {
+  if (B < 0) return fail(EMDB_ERR_INVALID, "B must be >= 0");
+  if (B == 0) return EMDB_OK;
+  if (!params || !X || !mu || !sd || !Z1 || !H1 || !Z2 || !H2 || !Y)
+    return fail(EMDB_ERR_INVALID, "NULL buffer");
+  emdb::MlpFwdParams p{params, X, mu, sd, B, Z1, H1, Z2, H2, Y};
+  cudaError_t e = emdb::launch_mlp_forward(p, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "mlp forward launch");
+  return EMDB_OK;
+}
+
+int emdb_mlp_backward(const float* params, const float* X, const float* mu, const float* sd,
+                      const float* Z1, const float* H1, const float* Z2, const float* H2,
+                      const float* Y, const float* T, int B, float* dY, float* dZ2, float* dZ1,
+                      float* grads, float* loss, void* stream) {
+  if (B <= 0) return fail(EMDB_ERR_INVALID, "B must be > 0");
+  if (!params || !X || !mu || !sd || !Z1 || !H1 || !Z2 || !H2 || !Y || !T || !dY || !dZ2 || !dZ1 ||
+      !grads || !loss)
+    return fail(EMDB_ERR_INVALID, "NULL buffer");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(loss, 0, sizeof(float), st);
+  if (e != cudaSuccess) return cuda_fail(e, "loss reset");
+  emdb::MlpBwdParams p{params, X, mu, sd, Z1, H1, Z2, H2, Y, T, B, dY, dZ2, dZ1, loss};
+  e = emdb::launch_mlp_backward(p, grads, st);
+  if (e != cudaSuccess) return cuda_fail(e, "mlp backward launch");
+  return EMDB_OK;
+}
+
+int emdb_mlp_adam(float* params, const float* grads, float* m, float* v, int n, float lr,
+                  float beta1, float beta2, float eps, int step, uint16_t* params_bf16,
+                  void* stream) {
+  if (n <= 0 || step < 1) return fail(EMDB_ERR_INVALID, "n must be > 0 and step >= 1");
+  if (!params || !grads || !m || !v) return fail(EMDB_ERR_INVALID, "NULL buffer");
+  cudaError_t e = emdb::launch_adam(params, grads, m, v, n, lr, beta1, beta2, eps, step,
+                                    reinterpret_cast<__nv_bfloat16*>(params_bf16),
+                                    (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "adam launch");
+  return EMDB_OK;
+}
+
+int emdb_mlp_infer_bf16(const uint16_t* params_bf16, const float* X, const float* mu,
+                        const float* sd, int B, float* Y, void* stream) {
+  if (B < 0) return fail(EMDB_ERR_INVALID, "B must be >= 0");
+  if (B == 0) return EMDB_OK;
+  if (!params_bf16 || !X || !mu || !sd || !Y) return fail(EMDB_ERR_INVALID, "NULL buffer");
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  emdb::MlpInferParams p{reinterpret_cast<const __nv_bfloat16*>(params_bf16), X, mu, sd, B, Y};
+  int tiles = (B + 31) / 32;
+  cudaError_t e = emdb::launch_mlp_infer(p, std::min(tiles, sms * 2), (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_fail(e, "mlp inference launch");
+  return EMDB_OK;
+}
+
+}  // extern "C"

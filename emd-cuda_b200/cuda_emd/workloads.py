@@ -63,7 +63,10 @@ def seismic_trace(rng: np.random.Generator, N: int, dt: float = DT_SEISMIC) -> n
     refl = np.zeros(N)
     pos = rng.integers(0, N, size=k)
     np.add.at(refl, pos, rng.laplace(0.0, 1.0, size=k))
-    sig = np.convolve(refl, _ricker(f, dt), mode="same")
+    w = _ricker(f, dt)
+    half = (w.shape[0] - 1) // 2
+    # centred crop of the full convolution (= mode "same" when N >= len(w))
+    sig = np.convolve(refl, w, mode="full")[half:half + N]
     noise = sosfilt(_bandpass_sos(dt), rng.normal(0.0, 1.0, size=N))
     ps = float(np.mean(sig * sig))
     pn = float(np.mean(noise * noise))

@@ -106,6 +106,40 @@ int emdb_envelope(emdb_plan* plan, const double* signals, const double* T, int b
  * (EMDB_STATUS_* bits) into *status. */
 int emdb_status(emdb_plan* plan, int* status, void* stream);
 
+/* ---- learned queue order (no reference counterpart: the reference launches
+ * one CTA per signal in index order, kernels.py:1366-1371).  All on the
+ * current CUDA device, asynchronous on `stream`. ---- */
+
+/* 32 float32 features per trace (length, zero-crossing and extrema rates,
+ * dyadic band energies, extrema density per eighth, moments):
+ * feat [batch, 32].  offsets = DEVICE int64 [batch+1], or NULL for a dense
+ * [batch, N] batch. */
+int emdb_features(const double* values, const int64_t* offsets, int batch, int N, float* feat,
+                  void* stream);
+
+/* MLP 32->128->128->2 (GELU).  Parameter block (float32, emdb_mlp_num_params()
+ * values): W1[32][128] b1[128] W2[128][128] b2[128] W3[128][2] b3[2].
+ * Inputs are raw features, standardised inside with mu/sd [32]. */
+int emdb_mlp_num_params(void);
+/* Training forward (FP32): keeps Z1/H1/Z2/H2 [B,128] for the backward, Y [B,2]. */
+int emdb_mlp_forward(const float* params, const float* X, const float* mu, const float* sd, int B,
+                     float* Z1, float* H1, float* Z2, float* H2, float* Y, void* stream);
+/* Backward of the mean squared error vs targets T [B,2]: grads (same layout
+ * as params), dY/dZ2/dZ1 scratch [B,2]/[B,128]/[B,128], *loss (device float)
+ * set to the batch MSE. */
+int emdb_mlp_backward(const float* params, const float* X, const float* mu, const float* sd,
+                      const float* Z1, const float* H1, const float* Z2, const float* H2,
+                      const float* Y, const float* T, int B, float* dY, float* dZ2, float* dZ1,
+                      float* grads, float* loss, void* stream);
+/* One Adam step (bias-corrected, step >= 1) on n parameters; if params_bf16
+ * is not NULL the updated weights are also written there as bfloat16. */
+int emdb_mlp_adam(float* params, const float* grads, float* m, float* v, int n, float lr,
+                  float beta1, float beta2, float eps, int step, uint16_t* params_bf16,
+                  void* stream);
+/* Inference with bfloat16 weights and FP32 accumulation: Y [B,2]. */
+int emdb_mlp_infer_bf16(const uint16_t* params_bf16, const float* X, const float* mu,
+                        const float* sd, int B, float* Y, void* stream);
+
 /* Message of the calling thread's last error ("" if none). */
 int emdb_last_error(char* buf, size_t len);
 
