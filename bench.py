@@ -42,13 +42,14 @@ METRIC = "EMD signals/s (FP64)"
 WORKLOADS = {
     "seismic16k": dict(n=16384, N=2048, desc="16384 seismic traces x 2048 samples, dt 2 ms"),
     "sinusoid256": dict(n=256, N=1024, desc="256 three-tone traces x 1024 samples"),
+    "seismic1k": dict(n=1024, N=2048, desc="1024 seismic traces x 2048 samples (profiling size)"),
 }
 
 
 def make_workload(name: str, rank: int = 0):
     from cuda_emd import workloads as W
     w = WORKLOADS[name]
-    if name == "seismic16k":
+    if name.startswith("seismic"):
         X = W.seismic_batch(w["n"], w["N"], seed=1 + 1000 * rank)
     else:
         X = W.sinusoid_batch(w["n"], w["N"], seed=0 + 1000 * rank)
@@ -169,6 +170,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=0, help="traces for the CPU leg (0 = auto)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--arena", type=int, default=0, help="shared-memory arena per CTA (0 = auto)")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -205,6 +207,9 @@ def main():
     emd = GPUBatchEMD(cfg)
     emd.warmup()
     launcher = emd._get_launcher()
+    if a.arena:
+        launcher._plan.set_arena(a.arena)
+    arena_used, ctas_per_sm, grid_max = launcher._plan.query(N)
 
     # ---- device-resident throughput ----
     for _ in range(a.warmup):
@@ -327,6 +332,7 @@ def main():
                        "batch_per_gpu": B, "N": N, "max_imfs": cfg.max_imfs,
                        "max_extrema": cfg.max_extrema, "max_iteration": cfg.max_iteration,
                        "queue": "FIFO persistent", "l2": "inputs+outputs larger than L2",
+                       "arena_bytes": arena_used, "ctas_per_sm": ctas_per_sm,
                        "overflow_traces": ovf, "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": a.steps,
@@ -337,38 +343,92 @@ def main():
         dist.destroy_process_group()
 
 
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libemd_ref.so")
+
+
 def run_reference(a, rank, world, pool, cores):
-    """The reference's algorithm on the host cores: the CPU oracle (the
-    reference ships no CPU path; its CUDA kernel needs CuPy, absent here)."""
+    """The reference's own emd_batch_kernel (kernels.py:834-1080, built from
+    kernels.py into oracle/_ref by oracle/build_ref.py: CuPy is absent, so
+    nvcc stands in for its NVRTC compile) on the same GPU and workload, with
+    the reference's launch geometry and per-call pool allocation + zero-fill
+    (kernels.py:1343-1372).  The CPU oracle on the host cores is reported as
+    its cpu_baseline.  Without the built library or a GPU, the CPU oracle is
+    the measured arm."""
     if rank != 0:
         return
     X = make_workload(a.workload, 0)
     B, N = X.shape
-    sample = a.cpu_sample or max(cores * 16, 64)
-    sample = min(sample, B)
-    for _ in range(max(0, min(a.warmup, 1))):
-        cpu_oracle_rate(X, pool, cores, min(cores, sample))
-    rates = []
-    t0 = time.perf_counter()
-    for k in range(a.steps):
-        r, n, wall = cpu_oracle_rate(X, pool, cores, sample)
-        rates.append(r)
-    tot = time.perf_counter() - t0
+    sample = min(a.cpu_sample or max(cores * 16, 64), B)
+    r, n, wall = cpu_oracle_rate(X, pool, cores, sample)
     pool.close()
-    value = statistics.mean(rates)
-    line = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "signals/s",
-        "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": round(B / value * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"], "batch_per_gpu": B,
-                   "N": N, "parallelism": "host cores"},
-        "cpu_baseline": {"value": round(value, 2), "unit": "signals/s", "cores": cores, "kind": "port",
-                         "sample": f"each step: first {sample} traces of the workload over {cores} "
-                                   f"processes ({tot:.1f} s for {a.steps} steps)"},
-        "e2e": {"value": round(value, 2), "unit": "signals/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
-    }
+    cpu = {"value": round(r, 2), "unit": "signals/s", "cores": cores, "kind": "port",
+           "sample": f"first {n} traces of the workload, NumPy oracle, {cores} processes, "
+                     f"{wall:.1f} s wall"}
+    import torch
+    line = {"impl": "reference", "metric": METRIC, "unit": "signals/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "cpu_baseline": cpu}
+    if os.path.isfile(REF_LIB) and torch.cuda.is_available():
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from refkernel import RefKernel
+        k = RefKernel("libemd_ref.so")
+        dev = torch.device("cuda", 0)
+        sig = torch.from_numpy(X).to(dev)
+        Tn = torch.arange(N, dtype=torch.float64, device=dev)
+        k.run_device(torch.zeros((1, 64), dtype=torch.float64, device=dev), Tn[:64])  # warmup()
+        for _ in range(a.warmup):
+            out = k.run_device(sig, Tn)
+            del out
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(a.steps):
+            out = k.run_device(sig, Tn)
+            del out
+        e1.record(st)
+        torch.cuda.synchronize()
+        el = e0.elapsed_time(e1) * 1e-3
+        value = B * a.steps / el
+        host_in = torch.from_numpy(X).pin_memory()
+        host_imfs = torch.empty((B, k.max_imfs, N), dtype=torch.float64).pin_memory()
+        h_n = torch.empty(B, dtype=torch.int32).pin_memory()
+        h_o = torch.empty(B, dtype=torch.int32).pin_memory()
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(a.steps):
+            d = host_in.to(dev, non_blocking=True)
+            imfs, nim, ovf, dn, de, dz = k.run_device(d, Tn)
+            bool(ovf.any())                      # emd.py:95 read-back
+            host_imfs.copy_(imfs, non_blocking=True)
+            h_n.copy_(nim, non_blocking=True)
+            h_o.copy_(ovf, non_blocking=True)
+            del imfs
+        e1.record(st)
+        torch.cuda.synchronize()
+        te = e0.elapsed_time(e1) * 1e-3
+        line.update({
+            "value": round(value, 2), "ms_per_step": round(el / a.steps * 1e3, 3),
+            "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
+                       "batch_per_gpu": B, "N": N,
+                       "reference_kernel": "emd_batch_kernel from kernels.py, nvcc -std=c++11 "
+                                           "sm_100a (oracle/_ref/libemd_ref.so); grid (batch,), "
+                                           "block 128, 57824 B dynamic smem",
+                       "parallelism": "one GPU"},
+            "e2e": {"value": round(B * a.steps / te, 2), "unit": "signals/s",
+                    "h2d_bytes_per_step": int(8 * B * N),
+                    "d2h_bytes_per_step": int(8 * B * k.max_imfs * N + 8 * B)},
+        })
+    else:
+        line.update({
+            "value": cpu["value"], "ms_per_step": round(B / max(r, 1e-9) * 1e3, 3),
+            "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
+                       "batch_per_gpu": B, "N": N, "parallelism": "host cores",
+                       "note": "reference kernel library not built here; CPU oracle measured"},
+            "e2e": {"value": cpu["value"], "unit": "signals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        })
     print(json.dumps(line), flush=True)
 
 

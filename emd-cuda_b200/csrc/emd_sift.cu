@@ -7,25 +7,28 @@
 //    atomic work queue (FIFO, or a caller-given order), so a long trace never
 //    holds a wave back and CSR batches of mixed length run in one launch;
 //  * the proto-IMF lives in shared memory for the whole decomposition; the
-//    running residue lives in the output rows (each row is written once,
-//    the residue row is rewritten once per IMF);
+//    running residue lives in the output rows (each row is written once, the
+//    residue row once more per IMF);
 //  * extrema: one warp-contiguous scan per sift pass computes ballot masks,
 //    zero-crossing counts and the serial-fallback trigger; the masks are
-//    compacted (popc ranks) straight into the knot arrays of both envelopes.
-//    The post-update scan of pass n is reused as the pre-scan of pass n+1
-//    (the reference scans the same data twice, kernels.py:930 vs 965);
-//  * boundary mirroring runs on one warp while the knot arrays are filled;
+//    compacted (popc ranks) straight into both envelopes' knot arrays, and
+//    their prefix counts give every sample its knot segment in O(1) when the
+//    knot list is strictly increasing (the reference binary-searches,
+//    kernels.py:722-726).  The post-update scan of pass n is reused as the
+//    pre-scan of pass n+1 (the reference scans the same data twice,
+//    kernels.py:930 vs 965);
+//  * boundary mirroring runs on one warp;
 //  * the upper and lower not-a-knot systems are solved concurrently by
 //    parallel cyclic reduction (ping-pong buffers, one barrier per level);
 //  * envelope evaluation, the mean update and the six stop-test partial
-//    sums are one fused pass; sums are formed in the reference's order
-//    (128 strided lanes + halving tree), and this file is compiled with
+//    sums are one fused pass; sums are formed in the reference's order (128
+//    strided lanes + halving tree) and this file is compiled with
 //    -fmad=false, so every value equals the reference algorithm's FP64
 //    result bit for bit (the CPU oracle checks this).
 //
-// Per-iteration knot/PCR storage is carved from the CTA's shared-memory
-// arena and spills to a per-CTA global slab only when a trace has more
-// knots than the arena holds.  All spin-free: no waits on other CTAs.
+// Per-pass knot/PCR storage is carved from the CTA's shared-memory arena; a
+// pass whose knots do not fit runs the same code on a per-CTA global slab.
+// Nothing here waits on another CTA.
 
 #include "emdb_internal.cuh"
 
@@ -50,8 +53,10 @@ struct Ctl {
   int w_max[kWarps], w_min[kWarps], w_zc[kWarps], w_zre[kWarps], w_trig[kWarps];
   int head[2][kMaxNbsym + 1];  // first NB+1 extrema indices per side (0 = max, 1 = min)
   int tail[2][kMaxNbsym + 1];  // tail[q][k] = index of extremum n_q-1-k
+  int mlist[4][kMaxNbsym + 1]; // mirrored index lists: lmax, lmin, rmax, rmin
+  int mcnt[4];
+  int lsym, rsym;
   int kbase[2], kcnt[2];
-  int mlist[4][kMaxNbsym + 1], mcnt[4], lsym, rsym;
   int dbg_n[kMaxImfsCap], dbg_e[kMaxImfsCap], dbg_z[kMaxImfsCap];
   int chunk_bad;
   double sums[8];
@@ -61,9 +66,9 @@ struct SmemLayout {
   Ctl* ctl;
   double* red;        // [6][128]
   double* imf;        // [N]
-  uint32_t* mmax;     // [nch]
+  uint32_t* mmax;     // [nch] ballot masks of the last extrema scan
   uint32_t* mmin;
-  uint16_t* pmax;     // per-chunk exclusive prefix within the warp's range
+  uint16_t* pmax;     // per-chunk exclusive prefix within the owning warp's range
   uint16_t* pmin;
   char* arena;        // knot arena start
   int arena_bytes;    // bytes left for the knot arena
@@ -80,7 +85,7 @@ __host__ __device__ inline size_t fixed_bytes(int N) {
   return b;
 }
 
-__device__ inline SmemLayout carve(char* base, int N, int arena_total) {
+__device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total) {
   SmemLayout L;
   size_t nch = (size_t)(N + 31) / 32;
   char* p = base;
@@ -96,46 +101,47 @@ __device__ inline SmemLayout carve(char* base, int N, int arena_total) {
   return L;
 }
 
-// Knot / PCR storage for one sift pass (both envelopes).
+// Knot / PCR storage for one sift pass (both envelopes).  After the last PCR
+// level only the b and d arrays of the final buffers are read, so the spline
+// moments M go into buffer 0's a (upper envelope) and c (lower) arrays.
 struct Knots {
   double* X[2];
   double* Y[2];
   double* M[2];
   double* P[2];   // ping-pong PCR buffers: a | b | c | d, each `cap` rows
-  int cap;        // PCR row capacity per buffer array
+  int cap;
 };
 
-__device__ inline size_t knot_bytes(int kc0, int kc1) {
-  // X, Y, M per side + 2 buffers x 4 arrays x (kc0+kc1) rows
-  return (size_t)(3 * (kc0 + kc1) + 8 * (kc0 + kc1)) * sizeof(double);
+__host__ __device__ inline size_t knot_bytes(int kc0, int kc1) {
+  return (size_t)(2 * (kc0 + kc1) + 8 * (kc0 + kc1)) * sizeof(double);
 }
 
-__device__ inline Knots place_knots(char* base, int kc0, int kc1) {
+__device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
   Knots K;
   double* p = reinterpret_cast<double*>(base);
   K.X[0] = p; p += kc0;
   K.Y[0] = p; p += kc0;
-  K.M[0] = p; p += kc0;
   K.X[1] = p; p += kc1;
   K.Y[1] = p; p += kc1;
-  K.M[1] = p; p += kc1;
   K.cap = kc0 + kc1;
   K.P[0] = p; p += 4 * K.cap;
   K.P[1] = p;
+  K.M[0] = K.P[0];
+  K.M[1] = K.P[0] + 2 * K.cap;
   return K;
 }
 
 struct TimeAxis {
   const double* T;
   bool arange;
-  __device__ inline double operator()(int i) const { return arange ? (double)i : T[i]; }
+  __device__ __forceinline__ double operator()(int i) const { return arange ? (double)i : T[i]; }
 };
 
 // ---------------------------------------------------------------------------
 // Extrema: count pass (find_extrema_parallel semantics, kernels.py:231-349,
 // with the serial scan's plateau rule, kernels.py:157-200).
 // ---------------------------------------------------------------------------
-__device__ void extrema_count(const SmemLayout& L, int N, int warp, int lane) {
+__device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int warp, int lane) {
   const double* imf = L.imf;
   int nch = (N + 31) >> 5;
   int c0 = (warp * nch) / kWarps, c1 = ((warp + 1) * nch) / kWarps;
@@ -191,13 +197,14 @@ struct ExtInfo {
   int n_zer;
   int off_max, off_min;   // this warp's rank offsets
   bool overflow;
+  bool trig;              // serial-fallback trigger (exact zeros / flat runs)
 };
 
 // After the count pass + barrier.  Reproduces the parallel/serial split of
 // find_extrema_parallel: without a fallback trigger the zero-crossing count is
 // sign changes only; with one, the serial count adds one per zero run that
 // ends before N (kernels.py:123-143, 273-276).
-__device__ ExtInfo extrema_totals(const SmemLayout& L, int N, int warp, int max_extrema) {
+__device__ __forceinline__ ExtInfo extrema_totals(const SmemLayout& L, int warp, int max_extrema) {
   const Ctl& C = *L.ctl;
   ExtInfo e;
   e.tot_max = e.tot_min = 0;
@@ -211,6 +218,7 @@ __device__ ExtInfo extrema_totals(const SmemLayout& L, int N, int warp, int max_
     zc += C.w_zc[w]; zre += C.w_zre[w];
     trig |= C.w_trig[w] != 0;
   }
+  e.trig = trig;
   if (!trig && C.chunk_bad) trig = true;
   e.n_zer = zc + (trig ? zre : 0);
   e.n_max = min(e.tot_max, max_extrema);
@@ -241,19 +249,15 @@ __device__ void chunk_fallback_check(const SmemLayout& L, int N, int tid) {
 
 // One extrema scan = count pass + totals.  Ends after a barrier with every
 // thread holding the same totals.
-__device__ ExtInfo extrema_scan(const SmemLayout& L, int N, int tid, int warp, int lane,
-                                int max_extrema) {
+__device__ __forceinline__ ExtInfo extrema_scan(const SmemLayout& L, int N, int tid, int warp,
+                                                int lane, int max_extrema) {
   extrema_count(L, N, warp, lane);
   if (tid == 0) L.ctl->chunk_bad = 0;
   __syncthreads();
-  ExtInfo e = extrema_totals(L, N, warp, max_extrema);
-  if (N > kThreads * 128 && L.imf[0] == 0.0) {
-    bool trig = false;
-    for (int w = 0; w < kWarps; ++w) trig |= L.ctl->w_trig[w] != 0;
-    if (!trig) {
-      chunk_fallback_check(L, N, tid);
-      e = extrema_totals(L, N, warp, max_extrema);
-    }
+  ExtInfo e = extrema_totals(L, warp, max_extrema);
+  if (N > kThreads * 128 && L.imf[0] == 0.0 && !e.trig) {
+    chunk_fallback_check(L, N, tid);
+    e = extrema_totals(L, warp, max_extrema);
   }
   return e;
 }
@@ -262,8 +266,9 @@ __device__ ExtInfo extrema_scan(const SmemLayout& L, int N, int tid, int warp, i
 // Knot fill: compacted true extrema -> X/Y at offset NB (both sides).
 // Returns this thread's "bad envelope sign" vote for true knots.
 // ---------------------------------------------------------------------------
-__device__ bool fill_true_knots(const SmemLayout& L, const Knots& K, const ExtInfo& e, int N,
-                                int NB, const TimeAxis& T, int warp, int lane) {
+__device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots& K,
+                                                const ExtInfo& e, int N, int NB,
+                                                const TimeAxis& T, int warp, int lane) {
   Ctl& C = *L.ctl;
   const double* imf = L.imf;
   int nch = (N + 31) >> 5;
@@ -272,27 +277,30 @@ __device__ bool fill_true_knots(const SmemLayout& L, const Knots& K, const ExtIn
   bool bad = false;
   for (int c = c0; c < c1; ++c) {
     uint32_t bm = L.mmax[c], bn = L.mmin[c];
-    if ((bm | bn) == 0u) continue;
     bool ismax = (bm >> lane) & 1u, ismin = (bn >> lane) & 1u;
     if (!(ismax || ismin)) continue;
     int i = (c << 5) + lane;
     int ii = i;
     double v = imf[i];
-    double dp = v - imf[i - 1], dn = imf[i + 1] - v;
-    if (!(dp * dn < 0.0)) {       // plateau extremum: report the run's midpoint
-      int j = i;
-      while (j + 1 < N && imf[j + 1] == v) ++j;
-      ii = (i + j) / 2;
+    if (e.trig) {
+      double dp = v - imf[i - 1], dn = imf[i + 1] - v;
+      if (!(dp * dn < 0.0)) {       // plateau extremum: report the run's midpoint
+        int j = i;
+        while (j + 1 < N && imf[j + 1] == v) ++j;
+        ii = (i + j) / 2;
+        v = imf[ii];
+      }
     }
     int q = ismax ? 0 : 1;
     int rank = q == 0 ? e.off_max + L.pmax[c] + __popc(bm & lt)
                       : e.off_min + L.pmin[c] + __popc(bn & lt);
     int nq = q == 0 ? e.n_max : e.n_min;
     if (rank < nq) {
-      double y = imf[ii];
-      K.X[q][NB + rank] = T(ii);
-      K.Y[q][NB + rank] = y;
-      bad |= q == 0 ? (y < 0.0) : (y > 0.0);
+      double* Xq = q == 0 ? K.X[0] : K.X[1];
+      double* Yq = q == 0 ? K.Y[0] : K.Y[1];
+      Xq[NB + rank] = T(ii);
+      Yq[NB + rank] = v;
+      bad |= q == 0 ? (v < 0.0) : (v > 0.0);
       if (rank <= NB) C.head[q][rank] = ii;
       int fe = nq - 1 - rank;
       if (fe <= NB) C.tail[q][fe] = ii;
@@ -303,112 +311,115 @@ __device__ bool fill_true_knots(const SmemLayout& L, const Knots& K, const ExtIn
 
 // ---------------------------------------------------------------------------
 // Boundary mirroring (mirror_one_side, kernels.py:360-558) for both sides.
-// Runs on warp 0; lane 0 makes the O(nbsym) decisions, lanes write knots.
-// Knot positions are strictly increasing whenever T is (the host checks T),
-// so the reference's adjacent-duplicate removal never drops a knot and is
-// not needed here.  Returns lane 0's "bad sign" vote for mirrored knots.
+// Lane 0 of warp 0 makes the O(nbsym) decisions into shared lists; the warp
+// then writes the mirrored knots.  Knot positions are strictly increasing
+// whenever T is (the host checks T), so the reference's adjacent-duplicate
+// removal never drops a knot and is not needed here.
 // ---------------------------------------------------------------------------
-__device__ bool mirror_both(const SmemLayout& L, const Knots& K, const ExtInfo& e, int N, int NB,
-                            const TimeAxis& T, int lane) {
+__device__ __forceinline__ int ind_of(const Ctl& C, int q, int n, int NB, int k) {
+  return k <= NB ? C.head[q][k] : C.tail[q][n - 1 - k];
+}
+
+__device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K, const ExtInfo& e,
+                                            int N, int NB, const TimeAxis& T, int lane) {
   Ctl& C = *L.ctl;
   const double* S = L.imf;
   const int nM = e.n_max, nm = e.n_min;
-  // list q: 0 lmax, 1 lmin, 2 rmax, 3 rmin
-  int lst[4][kMaxNbsym + 1];
-  int cnt[4];
-  int lsym = 0, rsym = 0;
   if (lane == 0) {
-    auto IM = [&](int k) { return k <= NB ? C.head[0][k] : C.tail[0][nM - 1 - k]; };
-    auto Im = [&](int k) { return k <= NB ? C.head[1][k] : C.tail[1][nm - 1 - k]; };
+    int* l0 = C.mlist[0];
+    int* l1 = C.mlist[1];
+    int* r0 = C.mlist[2];
+    int* r1 = C.mlist[3];
+    int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    int lsym, rsym;
+    const int im0 = ind_of(C, 0, nM, NB, 0), in0 = ind_of(C, 1, nm, NB, 0);
+    const int imL = ind_of(C, 0, nM, NB, nM - 1), inL = ind_of(C, 1, nm, NB, nm - 1);
     // ---- left bound ----
-    if (IM(0) < Im(0)) {
-      if (S[0] > S[Im(0)]) {
-        cnt[0] = 0; for (int k = min(nM, NB + 1) - 1; k >= 1; --k) lst[0][cnt[0]++] = IM(k);
-        cnt[1] = 0; for (int k = min(nm, NB) - 1; k >= 0; --k) lst[1][cnt[1]++] = Im(k);
-        lsym = IM(0);
+    if (im0 < in0) {
+      if (S[0] > S[in0]) {
+        for (int k = min(nM, NB + 1) - 1; k >= 1; --k) l0[c0++] = ind_of(C, 0, nM, NB, k);
+        for (int k = min(nm, NB) - 1; k >= 0; --k) l1[c1++] = ind_of(C, 1, nm, NB, k);
+        lsym = im0;
       } else {
-        cnt[0] = 0; for (int k = min(nM, NB) - 1; k >= 0; --k) lst[0][cnt[0]++] = IM(k);
-        cnt[1] = 0; for (int k = min(nm, NB - 1) - 1; k >= 0; --k) lst[1][cnt[1]++] = Im(k);
-        lst[1][cnt[1]++] = 0;
+        for (int k = min(nM, NB) - 1; k >= 0; --k) l0[c0++] = ind_of(C, 0, nM, NB, k);
+        for (int k = min(nm, NB - 1) - 1; k >= 0; --k) l1[c1++] = ind_of(C, 1, nm, NB, k);
+        l1[c1++] = 0;
         lsym = 0;
       }
     } else {
-      if (S[0] < S[IM(0)]) {
-        cnt[0] = 0; for (int k = min(nM, NB) - 1; k >= 0; --k) lst[0][cnt[0]++] = IM(k);
-        cnt[1] = 0; for (int k = min(nm, NB + 1) - 1; k >= 1; --k) lst[1][cnt[1]++] = Im(k);
-        lsym = Im(0);
+      if (S[0] < S[im0]) {
+        for (int k = min(nM, NB) - 1; k >= 0; --k) l0[c0++] = ind_of(C, 0, nM, NB, k);
+        for (int k = min(nm, NB + 1) - 1; k >= 1; --k) l1[c1++] = ind_of(C, 1, nm, NB, k);
+        lsym = in0;
       } else {
-        cnt[0] = 0; for (int k = min(nM, NB - 1) - 1; k >= 0; --k) lst[0][cnt[0]++] = IM(k);
-        lst[0][cnt[0]++] = 0;
-        cnt[1] = 0; for (int k = min(nm, NB) - 1; k >= 0; --k) lst[1][cnt[1]++] = Im(k);
+        for (int k = min(nM, NB - 1) - 1; k >= 0; --k) l0[c0++] = ind_of(C, 0, nM, NB, k);
+        l0[c0++] = 0;
+        for (int k = min(nm, NB) - 1; k >= 0; --k) l1[c1++] = ind_of(C, 1, nm, NB, k);
         lsym = 0;
       }
     }
     // ---- right bound ----
-    if (IM(nM - 1) < Im(nm - 1)) {
-      if (S[N - 1] < S[IM(nM - 1)]) {
-        cnt[2] = 0; for (int k = nM - 1; k >= max(nM - NB, 0); --k) lst[2][cnt[2]++] = IM(k);
-        cnt[3] = 0; for (int k = nm - 2; k >= max(nm - NB - 1, 0); --k) lst[3][cnt[3]++] = Im(k);
-        rsym = Im(nm - 1);
+    if (imL < inL) {
+      if (S[N - 1] < S[imL]) {
+        for (int k = nM - 1; k >= max(nM - NB, 0); --k) r0[c2++] = ind_of(C, 0, nM, NB, k);
+        for (int k = nm - 2; k >= max(nm - NB - 1, 0); --k) r1[c3++] = ind_of(C, 1, nm, NB, k);
+        rsym = inL;
       } else {
-        cnt[2] = 0; lst[2][cnt[2]++] = N - 1;
-        for (int k = max(nM - NB + 1, 0); k < nM; ++k) lst[2][cnt[2]++] = IM(k);
-        cnt[3] = 0; for (int k = nm - 1; k >= max(nm - NB, 0); --k) lst[3][cnt[3]++] = Im(k);
+        r0[c2++] = N - 1;
+        for (int k = max(nM - NB + 1, 0); k < nM; ++k) r0[c2++] = ind_of(C, 0, nM, NB, k);
+        for (int k = nm - 1; k >= max(nm - NB, 0); --k) r1[c3++] = ind_of(C, 1, nm, NB, k);
         rsym = N - 1;
       }
     } else {
-      if (S[N - 1] > S[Im(nm - 1)]) {
-        cnt[2] = 0; for (int k = nM - 2; k >= max(nM - NB - 1, 0); --k) lst[2][cnt[2]++] = IM(k);
-        cnt[3] = 0; for (int k = nm - 1; k >= max(nm - NB, 0); --k) lst[3][cnt[3]++] = Im(k);
-        rsym = IM(nM - 1);
+      if (S[N - 1] > S[inL]) {
+        for (int k = nM - 2; k >= max(nM - NB - 1, 0); --k) r0[c2++] = ind_of(C, 0, nM, NB, k);
+        for (int k = nm - 1; k >= max(nm - NB, 0); --k) r1[c3++] = ind_of(C, 1, nm, NB, k);
+        rsym = imL;
       } else {
-        cnt[2] = 0; for (int k = nM - 1; k >= max(nM - NB, 0); --k) lst[2][cnt[2]++] = IM(k);
-        cnt[3] = 0; lst[3][cnt[3]++] = N - 1;
-        for (int k = max(nm - NB + 1, 0); k < nm; ++k) lst[3][cnt[3]++] = Im(k);
+        for (int k = nM - 1; k >= max(nM - NB, 0); --k) r0[c2++] = ind_of(C, 0, nM, NB, k);
+        r1[c3++] = N - 1;
+        for (int k = max(nm - NB + 1, 0); k < nm; ++k) r1[c3++] = ind_of(C, 1, nm, NB, k);
         rsym = N - 1;
       }
     }
     // An empty list falls back to the whole index list (kernels.py:456-459,
     // 523-531); that only happens when the side has exactly one extremum,
     // so the whole list is that one index.
-    if (cnt[0] == 0) { lst[0][0] = IM(0); cnt[0] = 1; }
-    if (cnt[1] == 0) { lst[1][0] = Im(0); cnt[1] = 1; }
-    if (cnt[2] == 0) { lst[2][0] = IM(nM - 1); cnt[2] = 1; }
-    if (cnt[3] == 0) { lst[3][0] = Im(nm - 1); cnt[3] = 1; }
+    if (c0 == 0) l0[c0++] = im0;
+    if (c1 == 0) l1[c1++] = in0;
+    if (c2 == 0) r0[c2++] = imL;
+    if (c3 == 0) r1[c3++] = inL;
     // ---- mirrored point does not reach the boundary (kernels.py:469-503) ----
+    const double T0 = T(0), TN = T(N - 1);
     double tl = T(lsym);
-    double tlmin0 = 2.0 * tl - T(lst[1][0]);
-    double tlmax0 = 2.0 * tl - T(lst[0][0]);
-    double T0 = T(0), TN = T(N - 1);
-    if (tlmin0 > T0 || tlmax0 > T0) {
-      if (lsym == IM(0)) {
-        cnt[0] = 0; for (int k = min(nM, NB) - 1; k >= 0; --k) lst[0][cnt[0]++] = IM(k);
+    if (2.0 * tl - T(l1[0]) > T0 || 2.0 * tl - T(l0[0]) > T0) {
+      if (lsym == im0) {
+        c0 = 0;
+        for (int k = min(nM, NB) - 1; k >= 0; --k) l0[c0++] = ind_of(C, 0, nM, NB, k);
       } else {
-        cnt[1] = 0; for (int k = min(nm, NB) - 1; k >= 0; --k) lst[1][cnt[1]++] = Im(k);
+        c1 = 0;
+        for (int k = min(nm, NB) - 1; k >= 0; --k) l1[c1++] = ind_of(C, 1, nm, NB, k);
       }
       lsym = 0;
     }
     double tr = T(rsym);
-    double trmin = 2.0 * tr - T(lst[3][cnt[3] - 1]);
-    double trmax = 2.0 * tr - T(lst[2][cnt[2] - 1]);
-    if (trmin < TN || trmax < TN) {
-      if (rsym == IM(nM - 1)) {
-        cnt[2] = 0; for (int k = nM - 1; k >= max(nM - NB, 0); --k) lst[2][cnt[2]++] = IM(k);
+    if (2.0 * tr - T(r1[c3 - 1]) < TN || 2.0 * tr - T(r0[c2 - 1]) < TN) {
+      if (rsym == imL) {
+        c2 = 0;
+        for (int k = nM - 1; k >= max(nM - NB, 0); --k) r0[c2++] = ind_of(C, 0, nM, NB, k);
       } else {
-        cnt[3] = 0; for (int k = nm - 1; k >= max(nm - NB, 0); --k) lst[3][cnt[3]++] = Im(k);
+        c3 = 0;
+        for (int k = nm - 1; k >= max(nm - NB, 0); --k) r1[c3++] = ind_of(C, 1, nm, NB, k);
       }
       rsym = N - 1;
     }
-    C.kbase[0] = NB - cnt[0];
-    C.kbase[1] = NB - cnt[1];
-    C.kcnt[0] = cnt[0] + nM + cnt[2];
-    C.kcnt[1] = cnt[1] + nm + cnt[3];
-    for (int q = 0; q < 4; ++q) {
-      C.mcnt[q] = cnt[q];
-      for (int j = 0; j < cnt[q]; ++j) C.mlist[q][j] = lst[q][j];
-    }
+    C.mcnt[0] = c0; C.mcnt[1] = c1; C.mcnt[2] = c2; C.mcnt[3] = c3;
     C.lsym = lsym;
     C.rsym = rsym;
+    C.kbase[0] = NB - c0;
+    C.kbase[1] = NB - c1;
+    C.kcnt[0] = c0 + nM + c2;
+    C.kcnt[1] = c1 + nm + c3;
   }
   __syncwarp();
   // lanes write the mirrored knots: entry j of list q (0 lmax, 1 lmin, 2 rmax, 3 rmin)
@@ -424,8 +435,8 @@ __device__ bool mirror_both(const SmemLayout& L, const Knots& K, const ExtInfo& 
     double val = S[idx];
     int nside = side == 0 ? nM : nm;
     int slot = left ? (NB - cq + j) : (NB + nside + j);
-    K.X[side][slot] = pos;
-    K.Y[side][slot] = val;
+    (side == 0 ? K.X[0] : K.X[1])[slot] = pos;
+    (side == 0 ? K.Y[0] : K.Y[1])[slot] = val;
     bad |= side == 0 ? (val < 0.0) : (val > 0.0);
   }
   return bad;
@@ -434,8 +445,8 @@ __device__ bool mirror_both(const SmemLayout& L, const Knots& K, const ExtInfo& 
 // ---------------------------------------------------------------------------
 // Not-a-knot spline: reduced system + PCR + moments (kernels.py:607-697).
 // ---------------------------------------------------------------------------
-__device__ inline void setup_row(const double* x, const double* y, int n, int k, int m,
-                                 double& a, double& b, double& c, double& d) {
+__device__ __forceinline__ void setup_row(const double* x, const double* y, int n, int k, int m,
+                                          double& a, double& b, double& c, double& d) {
   if (k == 0) {
     double h0 = x[1] - x[0], h1 = x[2] - x[1];
     double rhs1 = 6.0 * ((y[2] - y[1]) / h1 - (y[1] - y[0]) / h0);
@@ -452,42 +463,38 @@ __device__ inline void setup_row(const double* x, const double* y, int n, int k,
   }
 }
 
-struct SideView {
-  const double* x;
-  const double* y;
-  const double* M;
-  int n;
-};
-
-__device__ void solve_splines(const Knots& K, const int kbase[2], const int kcnt[2], int tid) {
-  int m[2];
-  m[0] = kcnt[0] >= 4 ? kcnt[0] - 2 : 0;
-  m[1] = kcnt[1] >= 4 ? kcnt[1] - 2 : 0;
-  const int mt = m[0] + m[1];
+__device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kbase1, int kcnt0,
+                                              int kcnt1, int tid) {
+  const int m0 = kcnt0 >= 4 ? kcnt0 - 2 : 0;
+  const int m1 = kcnt1 >= 4 ? kcnt1 - 2 : 0;
+  const int mt = m0 + m1;
   const int cap = K.cap;
-  // setup -> P[0]
+  const double* x0b = K.X[0] + kbase0;
+  const double* x1b = K.X[1] + kbase1;
+  const double* y0b = K.Y[0] + kbase0;
+  const double* y1b = K.Y[1] + kbase1;
   for (int r = tid; r < mt; r += kThreads) {
-    int q = r < m[0] ? 0 : 1;
-    int k = q == 0 ? r : r - m[0];
-    const double* x = K.X[q] + kbase[q];
-    const double* y = K.Y[q] + kbase[q];
+    const bool s0 = r < m0;
+    const int k = s0 ? r : r - m0;
+    const double* x = s0 ? x0b : x1b;
+    const double* y = s0 ? y0b : y1b;
     double a, b, c, d;
-    setup_row(x, y, kcnt[q], k, m[q], a, b, c, d);
+    setup_row(x, y, s0 ? kcnt0 : kcnt1, k, s0 ? m0 : m1, a, b, c, d);
     double* P = K.P[0];
     P[r] = a; P[cap + r] = b; P[2 * cap + r] = c; P[3 * cap + r] = d;
   }
   __syncthreads();
-  int mmax = max(m[0], m[1]);
+  const int mmax = max(m0, m1);
   int cur = 0;
-  int fin[2] = {0, 0};
+  int fin0 = 0, fin1 = 0;
   for (int s = 1; s < mmax; s *= 2) {
-    const double* Pa = K.P[cur];
-    double* Pn = K.P[cur ^ 1];
+    const double* Pa = cur ? K.P[1] : K.P[0];
+    double* Pn = cur ? K.P[0] : K.P[1];
     for (int r = tid; r < mt; r += kThreads) {
-      int q = r < m[0] ? 0 : 1;
-      int mq = m[q];
+      const bool s0 = r < m0;
+      const int mq = s0 ? m0 : m1;
       if (s >= mq) continue;
-      int k = q == 0 ? r : r - m[0];
+      const int k = s0 ? r : r - m0;
       bool hl = k - s >= 0, hr = k + s < mq;
       int rl = r - s, rr = r + s;
       double ak = Pa[r], bk = Pa[cap + r], ck = Pa[2 * cap + r], dk = Pa[3 * cap + r];
@@ -506,29 +513,28 @@ __device__ void solve_splines(const Knots& K, const int kbase[2], const int kcnt
       Pn[cap + r] = bk - alpha * c_left - beta * a_right;
       Pn[3 * cap + r] = dk - alpha * d_left - beta * d_right;
     }
-    if (s < m[0]) fin[0] ^= 1;
-    if (s < m[1]) fin[1] ^= 1;
+    if (s < m0) fin0 ^= 1;
+    if (s < m1) fin1 ^= 1;
     cur ^= 1;
     __syncthreads();
   }
   // diagonal solve + end-moment recovery (M[0], M[n-1] by the owners of the end rows)
   for (int r = tid; r < mt; r += kThreads) {
-    int q = r < m[0] ? 0 : 1;
-    int k = q == 0 ? r : r - m[0];
-    int mq = m[q];
-    int n = kcnt[q];
-    const double* Pf = K.P[fin[q]];
-    double* M = K.M[q];
+    const bool s0 = r < m0;
+    const int k = s0 ? r : r - m0;
+    const int mq = s0 ? m0 : m1;
+    const int n = s0 ? kcnt0 : kcnt1;
+    const double* Pf = (s0 ? fin0 : fin1) ? K.P[1] : K.P[0];
+    double* M = s0 ? K.M[0] : K.M[1];
+    const double* x = s0 ? x0b : x1b;
     double Mk1 = Pf[3 * cap + r] / Pf[cap + r];
     M[k + 1] = Mk1;
     if (k == 0) {
-      const double* x = K.X[q] + kbase[q];
       double M2 = Pf[3 * cap + r + 1] / Pf[cap + r + 1];
       double h0 = x[1] - x[0], h1 = x[2] - x[1];
       M[0] = ((h0 + h1) * Mk1 - h0 * M2) / h1;
     }
     if (k == mq - 1) {
-      const double* x = K.X[q] + kbase[q];
       double Mnm3 = Pf[3 * cap + r - 1] / Pf[cap + r - 1];
       double hnm3 = x[n - 2] - x[n - 3], hnm2 = x[n - 1] - x[n - 2];
       M[n - 1] = ((hnm3 + hnm2) * Mk1 - hnm2 * Mnm3) / hnm3;
@@ -537,26 +543,27 @@ __device__ void solve_splines(const Knots& K, const int kbase[2], const int kcnt
   __syncthreads();
 }
 
-// Envelope value at t (kernels.py:702-734); `inr` reports the t-range mask.
-__device__ inline double eval_env(const SideView& s, double t, bool& inr) {
+struct SideView {
+  const double* x;
+  const double* y;
+  const double* M;
+  int n;          // knots
+  int nl, nt;     // mirrored-left and true knots
+};
+
+// Envelope value at t in knot segment lo (kernels.py:706-733).
+__device__ __forceinline__ double eval_seg(const SideView& s, double t, int lo) {
   const double* x = s.x;
   const double* y = s.y;
-  int n = s.n;
-  inr = !(t < x[0] || t > x[n - 1]);
-  if (n == 2) {
+  if (s.n == 2) {
     double slope = (y[1] - y[0]) / (x[1] - x[0]);
     return y[0] + slope * (t - x[0]);
   }
-  if (n == 3) {
+  if (s.n == 3) {
     double l0 = (t - x[1]) * (t - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
     double l1 = (t - x[0]) * (t - x[2]) / ((x[1] - x[0]) * (x[1] - x[2]));
     double l2 = (t - x[0]) * (t - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
     return y[0] * l0 + y[1] * l1 + y[2] * l2;
-  }
-  int lo = 0, hi = n - 2;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (x[mid] <= t) lo = mid; else hi = mid - 1;
   }
   double x0 = x[lo], x1 = x[lo + 1];
   double y0 = y[lo], y1 = y[lo + 1];
@@ -567,9 +574,32 @@ __device__ inline double eval_env(const SideView& s, double t, bool& inr) {
   return A * y0 + B * y1 + ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h) / 6.0;
 }
 
+// The reference's per-sample binary search (kernels.py:722-726).
+__device__ __forceinline__ int search_seg(const SideView& s, double t) {
+  int lo = 0, hi = s.n - 2;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (s.x[mid] <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Same answer in O(1) for a strictly increasing knot list: the number of knots
+// at or left of t, less one, where the true knots are counted from the last
+// extrema scan's ballot masks (prefix per chunk + popc within the chunk).
+__device__ __forceinline__ int count_seg(const SideView& s, double t, int cnt_true) {
+  int k = min(cnt_true, s.nt);
+  for (int j = 0; j < s.nl; ++j) k += s.x[j] <= t;
+  const double* xr = s.x + s.nl + s.nt;
+  for (int j = 0; j < s.n - s.nl - s.nt; ++j) k += xr[j] <= t;
+  int lo = k - 1;
+  lo = lo < 0 ? 0 : lo;
+  return lo > s.n - 2 ? s.n - 2 : lo;
+}
+
 // 128-lane tree of the reference (kernels.py:794-804), on warp 0, for a value
 // each thread has stored at red[q*128 + tid].  op 0: sum, 1: fmax, 2: fmin.
-__device__ inline double lane_tree(const double* red, int lane, int op) {
+__device__ __forceinline__ double lane_tree(const double* red, int lane, int op) {
   double v0 = red[lane], v1 = red[lane + 32], v2 = red[lane + 64], v3 = red[lane + 96];
   double r;
   if (op == 0) r = (v0 + v2) + (v1 + v3);
@@ -583,6 +613,97 @@ __device__ inline double lane_tree(const double* red, int lane, int op) {
     else r = fmin(r, o);
   }
   return r;
+}
+
+struct PassSums {
+  double sq, dsq, osq, std_, omax, omin;
+  bool bad;
+  bool oor;
+};
+
+__device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) {
+  double diff = nw - old;
+  ps.sq += nw * nw;
+  ps.dsq += diff * diff;
+  ps.osq += old * old;
+  double qd = diff / nw;
+  ps.std_ += qd * qd;
+  ps.omax = fmax(ps.omax, old);
+  ps.omin = fmin(ps.omin, old);
+}
+
+// One sift pass after the extrema scan of the current proto-IMF: knots,
+// mirroring, both splines, then the fused envelope / mean / update / partial
+// sums.  kSmem selects shared-memory knot storage (the common case) or the
+// per-CTA global slab, so each instantiation addresses one memory space.
+template <bool kSmem>
+__device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
+                                              int N, int NB, const TimeAxis& T, int tid, int warp,
+                                              int lane) {
+  Ctl& C = *L.ctl;
+  double* imf = L.imf;
+  const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
+  Knots K = place_knots(kSmem ? L.arena : slab, kc0, kc1);
+  PassSums ps;
+  bool bad = fill_true_knots(L, K, e, N, NB, T, warp, lane);
+  bad = __syncthreads_or(bad);
+  bool mbad = false;
+  if (warp == 0) mbad = mirror_both(L, K, e, N, NB, T, lane);
+  ps.bad = __syncthreads_or(bad || mbad) != 0;
+  const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
+  solve_splines(K, kb0, kb1, kn0, kn1, tid);
+
+  SideView sv0, sv1;
+  sv0.x = K.X[0] + kb0; sv0.y = K.Y[0] + kb0; sv0.M = K.M[0];
+  sv0.n = kn0; sv0.nl = NB - kb0; sv0.nt = e.n_max;
+  sv1.x = K.X[1] + kb1; sv1.y = K.Y[1] + kb1; sv1.M = K.M[1];
+  sv1.n = kn1; sv1.nl = NB - kb1; sv1.nt = e.n_min;
+
+  ps.sq = ps.dsq = ps.osq = ps.std_ = 0.0;
+  ps.omax = -1e30;
+  ps.omin = 1e30;
+  bool oor = false;
+  // O(1) segments need a strictly increasing knot list: true for nbsym <= 2
+  // without flat runs (plateau extrema sit at a run midpoint, not at the
+  // flagged sample).  Otherwise use the reference's binary search.
+  const bool fast = NB <= 2 && !e.trig;
+  const int nch = (N + 31) >> 5;
+  // chunk c = (tid>>5) + 4j is scanned by warp wc(c); its rank offset is woff[wc] + pre[c]
+  const int wm0 = C.w_max[0], wm1 = C.w_max[1], wm2 = C.w_max[2];
+  const int wn0 = C.w_min[0], wn1 = C.w_min[1], wn2 = C.w_min[2];
+  const int c1e = nch / kWarps, c2e = (2 * nch) / kWarps, c3e = (3 * nch) / kWarps;
+  const unsigned incl = lane == 31 ? kFull : ((2u << lane) - 1u);
+  for (int i = tid; i < N; i += kThreads) {
+    const double t = T(i);
+    int lo0 = 0, lo1 = 0;
+    if (fast) {
+      const int c = i >> 5;
+      // rank offset of the warp that scanned chunk c
+      const int o0 = (c >= c1e ? wm0 : 0) + (c >= c2e ? wm1 : 0) + (c >= c3e ? wm2 : 0);
+      const int o1 = (c >= c1e ? wn0 : 0) + (c >= c2e ? wn1 : 0) + (c >= c3e ? wn2 : 0);
+      const int ct0 = o0 + L.pmax[c] + __popc(L.mmax[c] & incl);
+      const int ct1 = o1 + L.pmin[c] + __popc(L.mmin[c] & incl);
+      if (sv0.n >= 4) lo0 = count_seg(sv0, t, ct0);
+      if (sv1.n >= 4) lo1 = count_seg(sv1, t, ct1);
+    } else {
+      if (sv0.n >= 4) lo0 = search_seg(sv0, t);
+      if (sv1.n >= 4) lo1 = search_seg(sv1, t);
+    }
+    oor |= (t < sv0.x[0]) || (t > sv0.x[sv0.n - 1]) ||
+           (t < sv1.x[0]) || (t > sv1.x[sv1.n - 1]);
+    const double emax = eval_seg(sv0, t, lo0);
+    const double emin = eval_seg(sv1, t, lo1);
+    const double mean = 0.5 * (emax + emin);
+    const double old = imf[i];
+    const double nw = old - mean;
+    imf[i] = nw;
+    accumulate(ps, old, nw);
+  }
+  // per-lane partial sums for the 128-lane trees
+  double* red = L.red;
+  red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
+  red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
+  return (ps.bad ? 1 : 0) | (oor ? 2 : 0);
 }
 
 }  // namespace
@@ -658,56 +779,15 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
           finished = true;
           break;
         }
-        // ---- knot storage for this pass ----
         const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
-        size_t need = knot_bytes(kc0, kc1);
-        char* kb = need <= (size_t)L.arena_bytes ? L.arena : slab;
-        Knots K = place_knots(kb, kc0, kc1);
-        // ---- true knots, then mirrored knots ----
-        bool bad = fill_true_knots(L, K, e, N, NB, T, warp, lane);
-        bad = __syncthreads_or(bad);
-        bool mbad = false;
-        if (warp == 0) mbad = mirror_both(L, K, e, N, NB, T, lane);
-        bad = __syncthreads_or(bad || mbad);
-        int kbase[2] = {C.kbase[0], C.kbase[1]};
-        int kcnt[2] = {C.kcnt[0], C.kcnt[1]};
-        // ---- both not-a-knot systems ----
-        solve_splines(K, kbase, kcnt, tid);
-        // ---- fused: envelopes, mean, update, stop-test partial sums ----
-        SideView sv[2];
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          sv[q].x = K.X[q] + kbase[q];
-          sv[q].y = K.Y[q] + kbase[q];
-          sv[q].M = K.M[q];
-          sv[q].n = kcnt[q];
-        }
-        double s_sq = 0.0, s_dsq = 0.0, s_osq = 0.0, s_std = 0.0;
-        double s_max = -1e30, s_min = 1e30;
-        bool oor = false;
-        for (int i = tid; i < N; i += kThreads) {
-          double t = T(i);
-          bool r0, r1;
-          double emax = eval_env(sv[0], t, r0);
-          double emin = eval_env(sv[1], t, r1);
-          oor |= !(r0 && r1);
-          double mean = 0.5 * (emax + emin);
-          double old = imf[i];
-          double nw = old - mean;
-          imf[i] = nw;
-          double diff = nw - old;
-          s_sq += nw * nw;
-          s_dsq += diff * diff;
-          s_osq += old * old;
-          double qd = diff / nw;
-          s_std += qd * qd;
-          s_max = fmax(s_max, old);
-          s_min = fmin(s_min, old);
-        }
-        stale |= oor;
+        int flags;
+        if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes)
+          flags = sift_pass<true>(L, slab, e, N, NB, T, tid, warp, lane);
+        else
+          flags = sift_pass<false>(L, slab, e, N, NB, T, tid, warp, lane);
+        const bool pass_bad = (flags & 1) != 0;
+        stale |= (flags & 2) != 0;
         double* red = L.red;
-        red[tid] = s_sq; red[128 + tid] = s_dsq; red[256 + tid] = s_osq;
-        red[384 + tid] = s_std; red[512 + tid] = s_max; red[640 + tid] = s_min;
         __syncthreads();
         if (warp == 0) {
           double a0 = lane_tree(red, lane, 0);
@@ -728,7 +808,7 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
         const int nzm2 = e.n_zer;
         const bool f2 = abs(extNo2 - nzm2) < 2;
         bool f1 = false;
-        if (!bad) {
+        if (!pass_bad) {
           double sum_new_sq = C.sums[0], diff_sq = C.sums[1], old_sq = C.sums[2];
           double std_sum = C.sums[3], omax = C.sums[4], omin = C.sums[5];
           if (sum_new_sq < kSumNewSqMin) f1 = false;
@@ -816,8 +896,8 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
     if (tid == 0) {
       p.n_imfs[b] = nim;
       p.overflow[b] = ovf ? 1 : 0;
-      if (stale) atomicOr(p.status, kStatusStaleEnvelope);
     }
+    if (stale) atomicOr(p.status, kStatusStaleEnvelope);
     for (int k = tid; k < MAXI; k += kThreads) {
       p.dbg_n[(int64_t)b * MAXI + k] = C.dbg_n[k];
       p.dbg_ext[(int64_t)b * MAXI + k] = C.dbg_e[k];
@@ -833,6 +913,50 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
 // reference scans with find_extrema_serial here; the extrema lists are the
 // same as the sift scan's (plateau rule included) and n_zer is not reported.
 // ---------------------------------------------------------------------------
+template <bool kSmem>
+__device__ __forceinline__ void envelope_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
+                                              int N, int NB, const TimeAxis& T, int tid, int warp,
+                                              int lane, double* emax_out, double* emin_out,
+                                              double* kp[2], double* kv[2], int mbuf, int nk[2],
+                                              int* status) {
+  Ctl& C = *L.ctl;
+  const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
+  Knots K = place_knots(kSmem ? L.arena : slab, kc0, kc1);
+  fill_true_knots(L, K, e, N, NB, T, warp, lane);
+  __syncthreads();
+  if (warp == 0) mirror_both(L, K, e, N, NB, T, lane);
+  __syncthreads();
+  const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
+  solve_splines(K, kb0, kb1, kn0, kn1, tid);
+  SideView sv[2];
+  sv[0].x = K.X[0] + kb0; sv[0].y = K.Y[0] + kb0; sv[0].M = K.M[0]; sv[0].n = kn0;
+  sv[0].nl = NB - kb0; sv[0].nt = e.n_max;
+  sv[1].x = K.X[1] + kb1; sv[1].y = K.Y[1] + kb1; sv[1].M = K.M[1]; sv[1].n = kn1;
+  sv[1].nl = NB - kb1; sv[1].nt = e.n_min;
+  nk[0] = kn0;
+  nk[1] = kn1;
+  const int kcnt[2] = {kn0, kn1};
+  bool oor = false;
+  for (int i = tid; i < N; i += kThreads) {
+    double t = T(i);
+    int lo0 = sv[0].n >= 4 ? search_seg(sv[0], t) : 0;
+    int lo1 = sv[1].n >= 4 ? search_seg(sv[1], t) : 0;
+    bool r0 = !(t < sv[0].x[0] || t > sv[0].x[sv[0].n - 1]);
+    bool r1 = !(t < sv[1].x[0] || t > sv[1].x[sv[1].n - 1]);
+    double a = eval_seg(sv[0], t, lo0);
+    double c = eval_seg(sv[1], t, lo1);
+    emax_out[i] = r0 ? a : 0.0;
+    emin_out[i] = r1 ? c : 0.0;
+    oor |= !(r0 && r1);
+  }
+  if (oor) atomicOr(status, kStatusStaleEnvelope);
+  for (int q = 0; q < 2; ++q)
+    for (int k = tid; k < mbuf; k += kThreads) {
+      kp[q][k] = k < kcnt[q] ? sv[q].x[k] : 0.0;
+      kv[q][k] = k < kcnt[q] ? sv[q].y[k] : 0.0;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) {
   extern __shared__ __align__(16) char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -865,7 +989,6 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
       continue;
     }
     SmemLayout L = carve(smem, N, p.arena_bytes);
-    Ctl& C = *L.ctl;
     for (int i = tid; i < N; i += kThreads) L.imf[i] = S[i];
     __syncthreads();
     ExtInfo e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
@@ -873,37 +996,12 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
     int nk[2] = {0, 0};
     if (!degenerate) {
       const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
-      char* kb = knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? L.arena : slab;
-      Knots K = place_knots(kb, kc0, kc1);
-      fill_true_knots(L, K, e, N, NB, T, warp, lane);
-      __syncthreads();
-      if (warp == 0) mirror_both(L, K, e, N, NB, T, lane);
-      __syncthreads();
-      int kbase[2] = {C.kbase[0], C.kbase[1]};
-      int kcnt[2] = {C.kcnt[0], C.kcnt[1]};
-      solve_splines(K, kbase, kcnt, tid);
-      SideView sv[2];
-      for (int q = 0; q < 2; ++q) {
-        sv[q].x = K.X[q] + kbase[q]; sv[q].y = K.Y[q] + kbase[q];
-        sv[q].M = K.M[q]; sv[q].n = kcnt[q];
-        nk[q] = kcnt[q];
-      }
-      bool oor = false;
-      for (int i = tid; i < N; i += kThreads) {
-        double t = T(i);
-        bool r0, r1;
-        double a = eval_env(sv[0], t, r0);
-        double c = eval_env(sv[1], t, r1);
-        emax_out[i] = r0 ? a : 0.0;
-        emin_out[i] = r1 ? c : 0.0;
-        oor |= !(r0 && r1);
-      }
-      if (oor) atomicOr(p.status, kStatusStaleEnvelope);
-      for (int q = 0; q < 2; ++q)
-        for (int k = tid; k < p.mbuf; k += kThreads) {
-          kp[q][k] = k < kcnt[q] ? sv[q].x[k] : 0.0;
-          kv[q][k] = k < kcnt[q] ? sv[q].y[k] : 0.0;
-        }
+      if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes)
+        envelope_pass<true>(L, slab, e, N, NB, T, tid, warp, lane, emax_out, emin_out, kp, kv,
+                            p.mbuf, nk, p.status);
+      else
+        envelope_pass<false>(L, slab, e, N, NB, T, tid, warp, lane, emax_out, emin_out, kp, kv,
+                             p.mbuf, nk, p.status);
     } else {
       for (int i = tid; i < N; i += kThreads) { emax_out[i] = 0.0; emin_out[i] = 0.0; }
       for (int q = 0; q < 2; ++q)
@@ -920,27 +1018,11 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
   }
 }
 
-cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(emd_envelope_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, arena_bytes);
-  if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_envelope_kernel, kThreads,
-                                                       arena_bytes);
-}
-
-cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(emd_envelope_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, p.arena_bytes);
-  if (e != cudaSuccess) return e;
-  emd_envelope_kernel<<<grid, kThreads, p.arena_bytes, stream>>>(p);
-  return cudaGetLastError();
-}
-
 size_t sift_fixed_smem(int N) { return fixed_bytes(N); }
 
 size_t sift_slab_bytes(int max_extrema, int nbsym) {
-  size_t kc = (size_t)max_extrema + 2 * (size_t)nbsym + 2;
-  return align16((3 * 2 * kc + 8 * 2 * kc) * sizeof(double));
+  int kc = max_extrema + 2 * nbsym + 2;
+  return align16(knot_bytes(kc, kc));
 }
 
 cudaError_t sift_occupancy(int arena_bytes, int* ctas_per_sm) {
@@ -956,6 +1038,22 @@ cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream) {
                                        p.arena_bytes);
   if (e != cudaSuccess) return e;
   emd_sift_kernel<<<grid, kThreads, p.arena_bytes, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(emd_envelope_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, arena_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_envelope_kernel, kThreads,
+                                                       arena_bytes);
+}
+
+cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(emd_envelope_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, p.arena_bytes);
+  if (e != cudaSuccess) return e;
+  emd_envelope_kernel<<<grid, kThreads, p.arena_bytes, stream>>>(p);
   return cudaGetLastError();
 }
 

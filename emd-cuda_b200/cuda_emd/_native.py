@@ -25,7 +25,8 @@ STATUS_TOO_LONG = 2
 # Every symbol include/emdb200.h declares (checked by the CPU test suite).
 EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_set_arena",
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
-           "emdb_last_error")
+           "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
+           "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16")
 
 
 class EmdbConfig(ctypes.Structure):

@@ -1,0 +1,246 @@
+"""Ragged (CSR) batches: shared-memory tiers, an autotuner for each tier's
+arena, and a CUDA-graph-captured multi-tier launch.
+
+Traces are grouped by length into tiers (N <= 1024, 2048, 4096, 8192, 16384,
+...).  Each tier is one persistent launch of the sift kernel over that tier's
+traces, with its own plan (work-queue ticket, status word, spill slab) and
+its own shared-memory arena: short traces get small arenas and more resident
+CTAs per SM, long traces get room for their proto-IMF and knots.  The tier
+launches are issued longest tier first on forked streams, so when a tier's
+queue drains, its SMs pick up the next tier's CTAs.  The whole sequence can
+be captured once into a CUDA graph and replayed.
+
+Queue order inside a tier is FIFO (trace index) or, given per-trace costs,
+longest-predicted-first.  Order never changes a result.
+
+The autotuner times every candidate arena (1..4 CTAs per SM, plus the
+minimum that fits) on a sample of each tier and caches the winner in a JSON
+file keyed by device, config and tier.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+from . import _native
+from .kernels import EMDKernelConfig
+
+TIER_EDGES = (1024, 2048, 4096, 8192, 16384, 32768)
+SMEM_PER_SM = 233472      # B200: 228 KB per SM
+CTA_RESERVED = 1024       # shared memory the runtime reserves per CTA
+DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "emd_b200_autotune.json")
+
+
+def tier_of(n: int) -> int:
+    for e in TIER_EDGES:
+        if n <= e:
+            return e
+    raise ValueError(f"trace length {n} exceeds the largest tier {TIER_EDGES[-1]}")
+
+
+def candidate_arenas(plan: _native.Plan, max_n: int) -> list[int]:
+    """Arena sizes worth trying for traces up to max_n: the largest arena
+    that keeps k CTAs per SM resident, k = 4..1, if it holds the trace."""
+    auto, _, _ = plan.query(max_n)
+    fixed_min = auto if auto > 0 else 0
+    out = []
+    for k in (4, 3, 2, 1):
+        a = (SMEM_PER_SM // k - CTA_RESERVED) & ~15
+        a = min(a, 232448)
+        if a >= fixed_min or (auto > 0 and a >= auto):
+            out.append(a)
+    if auto > 0 and auto not in out:
+        out.append(auto)
+    return sorted(set(out))
+
+
+class Tier:
+    def __init__(self, edge: int, idx: np.ndarray, cfg: EMDKernelConfig, device: int):
+        self.edge = edge
+        self.idx = idx                      # trace indices (host, int64)
+        self.max_n = 0
+        self.plan = _native.Plan(cfg.to_c(), device)
+        self.arena = 0
+
+    def set_arena(self, a: int) -> None:
+        self.arena = int(a)
+        self.plan.set_arena(self.arena)
+
+
+class RaggedRunner:
+    """Decompose CSR batches with per-tier launches (optionally graph-captured)."""
+
+    def __init__(self, config: EMDKernelConfig | None = None, device: int | None = None,
+                 cache_path: str | None = DEFAULT_CACHE, autotune: bool = True):
+        import torch
+        self.cfg = config or EMDKernelConfig()
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        self.cache_path = cache_path
+        self.autotune = autotune
+        self._tiers: dict[int, Tier] = {}
+        self._graph = None
+        self._graph_key = None
+        self._cache = self._load_cache()
+
+    # -- autotune cache ----------------------------------------------------------
+    def _key(self, edge: int) -> str:
+        import torch
+        name = torch.cuda.get_device_name(self.device)
+        c = self.cfg
+        return f"{name}|{c.max_extrema},{c.nbsym},{c.max_iteration},{c.max_imfs}|{edge}"
+
+    def _load_cache(self) -> dict:
+        if self.cache_path and os.path.isfile(self.cache_path):
+            try:
+                return json.load(open(self.cache_path))
+            except Exception:
+                return {}
+        return {}
+
+    def _save_cache(self) -> None:
+        if not self.cache_path:
+            return
+        os.makedirs(os.path.dirname(self.cache_path), exist_ok=True)
+        tmp = self.cache_path + ".tmp"
+        json.dump(self._cache, open(tmp, "w"), indent=1)
+        os.replace(tmp, self.cache_path)
+
+    # -- planning ----------------------------------------------------------------
+    def tiers_for(self, lengths: np.ndarray) -> list[Tier]:
+        edges = np.array([tier_of(int(n)) for n in lengths]) if lengths.size else np.zeros(0)
+        out = []
+        for e in sorted(set(edges.tolist()), reverse=True):   # longest tier first
+            idx = np.flatnonzero(edges == e)
+            t = self._tiers.get(e)
+            if t is None:
+                t = Tier(e, idx, self.cfg, self.device)
+                self._tiers[e] = t
+            t.idx = idx
+            t.max_n = int(lengths[idx].max())
+            out.append(t)
+        return out
+
+    def tune(self, values, offsets, lengths: np.ndarray, tiers: list[Tier], sample: int = 0) -> dict:
+        """Pick each tier's arena by timing the candidates on a sample of its traces."""
+        import torch
+        chosen = {}
+        for t in tiers:
+            key = self._key(t.edge)
+            if key in self._cache:
+                t.set_arena(self._cache[key]["arena"])
+                chosen[t.edge] = self._cache[key]
+                continue
+            cands = candidate_arenas(t.plan, t.edge)
+            if not cands:
+                raise ValueError(f"tier {t.edge} does not fit this device")
+            if len(cands) == 1 or not self.autotune:
+                t.set_arena(cands[-1] if not self.autotune else cands[0])
+                continue
+            n_s = sample or min(t.idx.size, 4 * 148 * 4)
+            sub = torch.from_numpy(t.idx[:n_s].astype(np.int32)).to(values.device)
+            res = {}
+            for a in cands:
+                t.set_arena(a)
+                outs = self._alloc_out(values, offsets)
+                self._launch_tier(t, values, offsets, sub, outs)       # warm
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                self._launch_tier(t, values, offsets, sub, outs)
+                e1.record()
+                e1.synchronize()
+                res[a] = e0.elapsed_time(e1)
+                del outs
+            best = min(res, key=res.get)
+            t.set_arena(best)
+            self._cache[key] = {"arena": best, "ms": res[best], "tried": {str(k): v for k, v in res.items()},
+                                "sample": int(n_s)}
+            chosen[t.edge] = self._cache[key]
+        self._save_cache()
+        return chosen
+
+    # -- launches ------------------------------------------------------------------
+    def _alloc_out(self, values, offsets):
+        import torch
+        B = offsets.shape[0] - 1
+        mi = self.cfg.max_imfs
+        dev = values.device
+        return (torch.empty(mi * values.shape[0], dtype=torch.float64, device=dev),
+                torch.empty(B, dtype=torch.int32, device=dev), torch.empty(B, dtype=torch.int32, device=dev),
+                torch.empty((B, mi), dtype=torch.int32, device=dev),
+                torch.empty((B, mi), dtype=torch.int32, device=dev),
+                torch.empty((B, mi), dtype=torch.int32, device=dev))
+
+    def _launch_tier(self, t: Tier, values, offsets, order_dev, outs, stream=None):
+        import torch
+        imfs, n_imfs, ovf, dn, de, dz = outs
+        st = (stream or torch.cuda.current_stream(values.device)).cuda_stream
+        _native.check(t.plan.L.emdb_run_ragged(
+            t.plan.handle, values.data_ptr(), offsets.data_ptr(), int(order_dev.shape[0]), int(t.edge),
+            None, 1, order_dev.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
+            dn.data_ptr(), de.data_ptr(), dz.data_ptr(), st), "emdb_run_ragged")
+
+    def prepare(self, values, offsets, cost=None):
+        """Host-side plan: tiers and per-tier queue orders (device int32)."""
+        import torch
+        off_h = offsets.cpu().numpy() if hasattr(offsets, "cpu") else np.asarray(offsets)
+        lengths = np.diff(off_h)
+        tiers = self.tiers_for(lengths)
+        self.tune(values, offsets, lengths, tiers)
+        orders = []
+        cost_h = None if cost is None else (cost.cpu().numpy() if hasattr(cost, "cpu") else np.asarray(cost))
+        for t in tiers:
+            idx = t.idx
+            if cost_h is not None:
+                idx = idx[np.argsort(-cost_h[idx], kind="stable")]
+            orders.append(torch.from_numpy(idx.astype(np.int32)).to(values.device))
+        if cost_h is not None:
+            # longest tier first already; within equal edges the heavier tier leads
+            pass
+        return tiers, orders
+
+    def run(self, values, offsets, cost=None, outs=None, use_graph: bool = False):
+        """Decompose; returns (imfs_csr, n_imfs, overflow, debug_n, debug_extno, debug_nzm)."""
+        import torch
+        tiers, orders = self.prepare(values, offsets, cost)
+        if outs is None:
+            outs = self._alloc_out(values, offsets)
+        main = torch.cuda.current_stream(values.device)
+        if use_graph:
+            key = (values.data_ptr(), offsets.data_ptr(), outs[0].data_ptr(),
+                   tuple(int(o.data_ptr()) for o in orders), tuple(t.arena for t in tiers))
+            if self._graph is None or self._graph_key != key:
+                self._issue(tiers, orders, values, offsets, outs, main)   # warm: allocs outside capture
+                torch.cuda.synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._issue(tiers, orders, values, offsets, outs, torch.cuda.current_stream())
+                self._graph, self._graph_key = g, key
+                self._graph_keep = (orders, outs, values, offsets)
+            self._graph.replay()
+        else:
+            self._issue(tiers, orders, values, offsets, outs, main)
+        return outs
+
+    def _issue(self, tiers, orders, values, offsets, outs, main):
+        import torch
+        streams = getattr(self, "_streams", None)
+        if streams is None or len(streams) < len(tiers):
+            self._streams = streams = [torch.cuda.Stream(values.device) for _ in range(max(len(tiers), 1))]
+        for t, o, s in zip(tiers, orders, streams):
+            s.wait_stream(main)
+            with torch.cuda.stream(s):
+                self._launch_tier(t, values, offsets, o, outs, stream=s)
+        for s in streams[:len(tiers)]:
+            main.wait_stream(s)
+
+    def check_status(self) -> None:
+        import torch
+        for t in self._tiers.values():
+            st = t.plan.status(torch.cuda.current_stream(self.device).cuda_stream)
+            if st & _native.STATUS_TOO_LONG:
+                raise ValueError("a trace did not fit its tier's shared-memory arena")
+            if st & _native.STATUS_STALE_ENVELOPE:
+                raise RuntimeError("a sample fell outside the envelope knot span")

@@ -178,3 +178,48 @@ def test_live_reference_kernel_cfg1_subsample():
     rng = np.ptp(X, axis=1)
     err = np.abs(mine[0] - stock[0]).max(axis=(1, 2))
     assert np.all(err <= IMF_RTOL * rng)
+
+
+@pytest.mark.parametrize("nbsym", [1, 3])
+def test_nbsym_variants_match_oracle(nbsym):
+    """nbsym != 2: nbsym=3 yields unsorted right-boundary knot lists (the
+    reference's own ordering), which the kernel evaluates with the reference's
+    binary search; both must equal the oracle bit for bit."""
+    from cuda_emd import EMDKernelConfig, workloads as W
+    from oracle import emd_oracle as O
+    X = W.sinusoid_batch(8, 512, seed=200 + nbsym)
+    T = np.arange(512, dtype=np.float64)
+    cfg = EMDKernelConfig(nbsym=nbsym)
+    imfs, n_imfs, ovf, dn, de, dz = _run_np(cfg, X, T)
+    ocfg = O.OracleConfig(nbsym=nbsym)
+    for b in range(X.shape[0]):
+        r = O.emd_signal(X[b], T, ocfg)
+        assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
+        np.testing.assert_array_equal(dn[b], r.debug_n)
+        assert _sha(imfs[b]) == _sha(r.imfs), (nbsym, b)
+
+
+@pytest.mark.parametrize("arena", [0, 26000, 232448])
+def test_arena_sizes_same_results(arena):
+    """Knot storage in shared memory or spilled to the global slab gives the
+    same bits (small arena forces the slab path)."""
+    import torch
+    from cuda_emd import EMDKernelConfig, workloads as W
+    X = W.seismic_batch(24, 2048, seed=300)
+    L = EMDKernelConfig().build()
+    ref = [o.cpu() for o in L.run(torch.from_numpy(X).cuda(), None)]
+    if arena:
+        L._plan.set_arena(arena)
+    out = [o.cpu() for o in L.run(torch.from_numpy(X).cuda(), None)]
+    L.check_status()
+    for a, b in zip(ref, out):
+        assert torch.equal(a, b)
+
+
+def test_arena_too_small_raises():
+    import torch
+    from cuda_emd import EMDKernelConfig
+    L = EMDKernelConfig().build()
+    L._plan.set_arena(20000)
+    with pytest.raises(ValueError):
+        L.run(torch.zeros((2, 2048), dtype=torch.float64, device="cuda"), None)
