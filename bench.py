@@ -43,6 +43,9 @@ WORKLOADS = {
     "seismic16k": dict(n=16384, N=2048, desc="16384 seismic traces x 2048 samples, dt 2 ms"),
     "sinusoid256": dict(n=256, N=1024, desc="256 three-tone traces x 1024 samples"),
     "seismic1k": dict(n=1024, N=2048, desc="1024 seismic traces x 2048 samples (profiling size)"),
+    "ragged64k": dict(n=65536, lo=256, hi=8192,
+                      desc="65536 mixed traces, N log-uniform [256, 8192] (60% seismic, 38% "
+                           "three-tone, 2% chirp), CSR; plain FIFO vs learned longest-first"),
 }
 
 
@@ -171,6 +174,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--arena", type=int, default=0, help="shared-memory arena per CTA (0 = auto)")
+    ap.add_argument("--variant", type=int, default=0, help="kernel register variant: min CTAs/SM")
+    ap.add_argument("--train-traces", type=int, default=200000, help="ragged64k: MLP training set")
+    ap.add_argument("--eval-traces", type=int, default=0, help="ragged64k: batch size (0 = 65536)")
+    ap.add_argument("--epochs", type=int, default=20)
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -187,6 +194,9 @@ def main():
 
     if a.impl == "reference":
         run_reference(a, rank, world, pool, cores)
+        return
+    if a.workload == "ragged64k":
+        run_ragged(a, rank, world, pool, cores)
         return
 
     import torch
@@ -207,6 +217,8 @@ def main():
     emd = GPUBatchEMD(cfg)
     emd.warmup()
     launcher = emd._get_launcher()
+    if a.variant:
+        launcher._plan.set_variant(a.variant)
     if a.arena:
         launcher._plan.set_arena(a.arena)
     arena_used, ctas_per_sm, grid_max = launcher._plan.query(N)
@@ -219,6 +231,9 @@ def main():
     n_imfs, dbg_n, dbg_ext = out[1].cpu().numpy(), out[3].cpu().numpy(), out[4].cpu().numpy()
     ovf = int(out[2].sum().item())
     del out
+    launcher._plan.counters(reset=True)
+    launcher.run(sig, None)
+    passes_step, spilled_step = launcher._plan.counters(reset=True)
     flops_per_step = algorithmic_flops(N, n_imfs, dbg_n, dbg_ext)
     hbm_bytes_per_step = 8.0 * B * N + 8.0 * B * cfg.max_imfs * N
 
@@ -333,6 +348,8 @@ def main():
                        "max_extrema": cfg.max_extrema, "max_iteration": cfg.max_iteration,
                        "queue": "FIFO persistent", "l2": "inputs+outputs larger than L2",
                        "arena_bytes": arena_used, "ctas_per_sm": ctas_per_sm,
+                       "sift_passes_per_step": passes_step,
+                       "spilled_pass_frac": round(spilled_step / max(passes_step, 1), 4),
                        "overflow_traces": ovf, "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "gpu_launches": a.steps,
@@ -429,6 +446,151 @@ def run_reference(a, rank, world, pool, cores):
             "e2e": {"value": cpu["value"], "unit": "signals/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
         })
+    print(json.dumps(line), flush=True)
+
+
+
+# ---------------------------------------------------------------------------
+# Ragged batch: plain FIFO tiers vs learned longest-predicted-first order
+# ---------------------------------------------------------------------------
+
+def _gen_ragged_chunk(args):
+    n, lo, hi, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "emd-cuda_b200"))
+    from cuda_emd import workloads as W
+    vals, offs, kinds = W.ragged_mix(n, lo=lo, hi=hi, seed=seed)
+    return vals, np.diff(offs)
+
+
+def gen_ragged(pool, n: int, lo: int, hi: int, seed: int, chunk: int = 2048):
+    """Deterministic CSR batch built from independently seeded chunks."""
+    parts = [(min(chunk, n - s), lo, hi, seed * 100003 + k)
+             for k, s in enumerate(range(0, n, chunk))]
+    res = pool.map(_gen_ragged_chunk, parts) if pool is not None else [_gen_ragged_chunk(p) for p in parts]
+    vals = np.concatenate([r[0] for r in res])
+    lens = np.concatenate([r[1] for r in res])
+    offs = np.zeros(lens.shape[0] + 1, dtype=np.int64)
+    np.cumsum(lens, out=offs[1:])
+    return vals, offs
+
+
+def run_ragged(a, rank, world, pool, cores):
+    import torch
+    from cuda_emd import EMDKernelConfig
+    from cuda_emd import scheduler as S
+    from cuda_emd.ragged import RaggedRunner
+    w = WORKLOADS["ragged64k"]
+    n_eval = a.eval_traces or w["n"]
+    t0 = time.perf_counter()
+    ev_vals, ev_offs = gen_ragged(pool, n_eval, w["lo"], w["hi"], seed=2 + 1000 * rank)
+    tr_vals, tr_offs = gen_ragged(pool, a.train_traces, w["lo"], w["hi"], seed=3 + 1000 * rank)
+    gen_s = time.perf_counter() - t0
+    if pool is not None:
+        pool.close()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfg = EMDKernelConfig.for_device(local)
+    v = torch.from_numpy(ev_vals).to(dev)
+    o = torch.from_numpy(ev_offs).to(dev)
+    B = n_eval
+    runner = RaggedRunner(cfg, device=local)
+
+    def timed(cost, steps, warm):
+        outs = runner.run(v, o, cost=cost, use_graph=True)
+        for _ in range(max(warm - 1, 0)):
+            outs = runner.run(v, o, cost=cost, outs=outs, use_graph=True)
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            outs = runner.run(v, o, cost=cost, outs=outs, use_graph=True)
+        e1.record(st)
+        torch.cuda.synchronize()
+        runner.check_status()
+        return outs, e0.elapsed_time(e1) * 1e-3 / steps
+
+    # plain: tiers, FIFO inside each tier
+    plain_out, plain_s = timed(None, a.steps, a.warmup)
+    plain_copy = [x.clone() for x in plain_out]
+    # labels for the cost model from the plain method on the training set
+    tv = torch.from_numpy(tr_vals).to(dev)
+    to = torch.from_numpy(tr_offs).to(dev)
+    tl0 = time.perf_counter()
+    tr_out = runner.run(tv, to)
+    torch.cuda.synchronize()
+    label_s = time.perf_counter() - tl0
+    labels = S.labels_from_debug(tr_out[3], tr_out[1])
+    del tr_out
+    feats_tr = S.features(tv, to)
+    cm = S.CostModel(local, seed=0)
+    tt0 = time.perf_counter()
+    hist = cm.fit(feats_tr, labels, epochs=a.epochs, batch=4096, lr=1e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - tt0
+    del tv, to, feats_tr
+    torch.cuda.empty_cache()
+    # learned order on the evaluation batch (features + BF16 inference inside the timing)
+    lens = o[1:] - o[:-1]
+    fe0 = torch.cuda.Event(enable_timing=True); fe1 = torch.cuda.Event(enable_timing=True)
+    fe0.record()
+    feats = S.features(v, o)
+    fm = torch.cuda.Event(enable_timing=True)
+    fm.record()
+    cost = S.predicted_cost(cm, feats, lens)
+    fe1.record()
+    torch.cuda.synchronize()
+    predict_s = fe0.elapsed_time(fe1) * 1e-3
+    feat_ms, infer_ms = fe0.elapsed_time(fm), fm.elapsed_time(fe1)
+    learned_out, learned_s = timed(cost, a.steps, a.warmup)
+    same = all(torch.equal(x, y) for x, y in zip(plain_copy, learned_out))
+    truth = S.labels_from_debug(plain_copy[3], plain_copy[1])
+    pred = cm.predict(feats)
+    mae_log2_passes = float((pred[:, 0] - truth[:, 0]).abs().mean())
+    passes_true = torch.exp2(truth[:, 0]) - 1
+    passes_pred = (torch.exp2(pred[:, 0]) - 1).clamp(min=0)
+    mae_passes = float((passes_pred - passes_true).abs().mean())
+    mae_nimfs = float((pred[:, 1] - truth[:, 1]).abs().mean())
+    tiers = {}
+    for t in runner._tiers.values():
+        t.plan.counters(reset=True)
+    runner.run(v, o, cost=cost, use_graph=True)
+    torch.cuda.synchronize()
+    for t in runner._tiers.values():
+        ps, sp = t.plan.counters(reset=True)
+        sub = torch.from_numpy(t.idx.astype(np.int32)).to(dev)
+        outs = runner._alloc_out(v, o)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        runner._launch_tier(t, v, o, sub, outs)
+        e1.record()
+        e1.synchronize()
+        tiers[str(t.edge)] = {"traces": int(t.idx.size), "arena": t.arena, "variant": t.variant,
+                              "passes": ps, "spilled_frac": round(sp / max(ps, 1), 4),
+                              "alone_ms": round(e0.elapsed_time(e1), 2)}
+        del outs
+    value = B / (learned_s + predict_s)
+    line = {
+        "metric": METRIC + " learned-scheduled vs plain", "value": round(value, 2),
+        "unit": "signals/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round((learned_s + predict_s) * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": "ragged64k", "desc": w["desc"], "batch_per_gpu": B,
+                   "samples": int(ev_offs[-1]), "tiers": tiers, "graph": True},
+        "plain": {"value": round(B / plain_s, 2), "ms_per_step": round(plain_s * 1e3, 3)},
+        "learned": {"value": round(value, 2), "ms_per_step": round(learned_s * 1e3, 3),
+                    "predict_ms": round(predict_s * 1e3, 3), "features_ms": round(feat_ms, 3),
+                    "infer_ms": round(infer_ms, 3),
+                    "speedup_vs_plain": round(plain_s / (learned_s + predict_s), 4),
+                    "bit_identical_to_fifo": bool(same)},
+        "cost_model": {"train_traces": a.train_traces, "epochs": a.epochs,
+                       "loss_first": round(hist[0], 5), "loss_last": round(hist[-1], 5),
+                       "train_s": round(train_s, 3), "label_s": round(label_s, 3),
+                       "mae_log2_passes": round(mae_log2_passes, 4),
+                       "mae_passes": round(mae_passes, 2), "mae_n_imfs": round(mae_nimfs, 4)},
+        "gen_s": round(gen_s, 1), "gpu_launches": a.steps * len(tiers),
+    }
     print(json.dumps(line), flush=True)
 
 

@@ -32,6 +32,23 @@
 
 #include "emdb_internal.cuh"
 
+// Tuning knobs (compile-time; results are identical for every setting):
+//  EMDB_EVAL_PAIR  evaluate two samples per loop trip in the fused pass
+//  EMDB_PCR_PAIR   update two PCR rows per loop trip
+//  EMDB_FAST_DIV   reciprocal-based correctly rounded division in evaluation
+// Measured on B200 (cfg1, 16,384 x 2048): all three off is fastest -- the
+// hardware-seeded FP64 division is already short, and the paired loops raise
+// register pressure more than they add overlap.
+#ifndef EMDB_EVAL_PAIR
+#define EMDB_EVAL_PAIR 0
+#endif
+#ifndef EMDB_PCR_PAIR
+#define EMDB_PCR_PAIR 0
+#endif
+#ifndef EMDB_FAST_DIV
+#define EMDB_FAST_DIV 0
+#endif
+
 namespace emdb {
 
 namespace {
@@ -103,11 +120,13 @@ __device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total) 
 
 // Knot / PCR storage for one sift pass (both envelopes).  After the last PCR
 // level only the b and d arrays of the final buffers are read, so the spline
-// moments M go into buffer 0's a (upper envelope) and c (lower) arrays.
+// moments M go into buffer 0's a (upper envelope) and c (lower) arrays and the
+// segment reciprocals R into buffer 1's a and c arrays.
 struct Knots {
   double* X[2];
   double* Y[2];
   double* M[2];
+  double* R[2];   // RN(1/h) per knot segment, in buffer 1's a / c arrays
   double* P[2];   // ping-pong PCR buffers: a | b | c | d, each `cap` rows
   int cap;
 };
@@ -128,8 +147,33 @@ __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
   K.P[1] = p;
   K.M[0] = K.P[0];
   K.M[1] = K.P[0] + 2 * K.cap;
+  K.R[0] = K.P[1];
+  K.R[1] = K.P[1] + 2 * K.cap;
   return K;
 }
+
+// Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 1990):
+// if y is within half an ulp of 1/b and q within one ulp of a/b, then with the
+// exact remainder r = a - b*q (one FMA), RN(q + r*y) = RN(a/b).  q0 = RN(a*y)
+// can be 1.5 ulp off, so one correction step first brings it within one ulp,
+// the second rounds correctly.  Operands whose remainders or quotient could
+// underflow or overflow (|a| or |a*y| outside [2^-900, 2^900], zeros, inf,
+// NaN) take the division.
+// Checked bit for bit against the hardware division by emdb_check_division.
+__device__ __noinline__ double div_slow(double a, double b) { return a / b; }
+
+__device__ __forceinline__ double div_rn(double a, double b, double y) {
+  const double q0 = a * y;
+  const double e0 = fma(-q0, b, a);
+  const double q1 = fma(e0, y, q0);
+  const double e1 = fma(-q1, b, a);
+  const double q2 = fma(e1, y, q1);
+  const double aa = fabs(a), qa = fabs(q0);
+  if (aa > 0x1p-900 && aa < 0x1p+900 && qa > 0x1p-900 && qa < 0x1p+900) return q2;
+  return div_slow(a, b);
+}
+constexpr double kInv6 = 1.0 / 6.0;   // RN(1/6), folded at compile time
 
 struct TimeAxis {
   const double* T;
@@ -463,6 +507,27 @@ __device__ __forceinline__ void setup_row(const double* x, const double* y, int 
   }
 }
 
+__device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* __restrict__ Pn,
+                                        int cap, int r, int k, int s, int mq) {
+  const bool hl = k - s >= 0, hr = k + s < mq;
+  const int rl = r - s, rr = r + s;
+  const double ak = Pa[r], bk = Pa[cap + r], ck = Pa[2 * cap + r], dk = Pa[3 * cap + r];
+  const double b_left = hl ? Pa[cap + rl] : 1.0;
+  const double b_right = hr ? Pa[cap + rr] : 1.0;
+  const double alpha = hl ? ak / b_left : 0.0;
+  const double beta = hr ? ck / b_right : 0.0;
+  const double a_left = hl ? Pa[rl] : 0.0;
+  const double c_left = hl ? Pa[2 * cap + rl] : 0.0;
+  const double d_left = hl ? Pa[3 * cap + rl] : 0.0;
+  const double a_right = hr ? Pa[rr] : 0.0;
+  const double c_right = hr ? Pa[2 * cap + rr] : 0.0;
+  const double d_right = hr ? Pa[3 * cap + rr] : 0.0;
+  Pn[r] = -alpha * a_left;
+  Pn[2 * cap + r] = -beta * c_right;
+  Pn[cap + r] = bk - alpha * c_left - beta * a_right;
+  Pn[3 * cap + r] = dk - alpha * d_left - beta * d_right;
+}
+
 __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kbase1, int kcnt0,
                                               int kcnt1, int tid) {
   const int m0 = kcnt0 >= 4 ? kcnt0 - 2 : 0;
@@ -488,35 +553,30 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
   int cur = 0;
   int fin0 = 0, fin1 = 0;
   for (int s = 1; s < mmax; s *= 2) {
-    const double* Pa = cur ? K.P[1] : K.P[0];
-    double* Pn = cur ? K.P[0] : K.P[1];
-    for (int r = tid; r < mt; r += kThreads) {
-      const bool s0 = r < m0;
-      const int mq = s0 ? m0 : m1;
-      if (s >= mq) continue;
-      const int k = s0 ? r : r - m0;
-      bool hl = k - s >= 0, hr = k + s < mq;
-      int rl = r - s, rr = r + s;
-      double ak = Pa[r], bk = Pa[cap + r], ck = Pa[2 * cap + r], dk = Pa[3 * cap + r];
-      double b_left = hl ? Pa[cap + rl] : 1.0;
-      double b_right = hr ? Pa[cap + rr] : 1.0;
-      double alpha = hl ? ak / b_left : 0.0;
-      double beta = hr ? ck / b_right : 0.0;
-      double a_left = hl ? Pa[rl] : 0.0;
-      double c_left = hl ? Pa[2 * cap + rl] : 0.0;
-      double d_left = hl ? Pa[3 * cap + rl] : 0.0;
-      double a_right = hr ? Pa[rr] : 0.0;
-      double c_right = hr ? Pa[2 * cap + rr] : 0.0;
-      double d_right = hr ? Pa[3 * cap + rr] : 0.0;
-      Pn[r] = -alpha * a_left;
-      Pn[2 * cap + r] = -beta * c_right;
-      Pn[cap + r] = bk - alpha * c_left - beta * a_right;
-      Pn[3 * cap + r] = dk - alpha * d_left - beta * d_right;
+    const double* __restrict__ Pa = cur ? K.P[1] : K.P[0];
+    double* __restrict__ Pn = cur ? K.P[0] : K.P[1];
+    // two rows per trip: independent division chains overlap
+    for (int r = tid; r < mt; r += (1 + EMDB_PCR_PAIR) * kThreads) {
+      const int r2 = EMDB_PCR_PAIR ? r + kThreads : mt;
+      {
+        const bool s0 = r < m0;
+        const int mq = s0 ? m0 : m1;
+        if (s < mq) pcr_row(Pa, Pn, cap, r, s0 ? r : r - m0, s, mq);
+      }
+      if (r2 < mt) {
+        const bool s0 = r2 < m0;
+        const int mq = s0 ? m0 : m1;
+        if (s < mq) pcr_row(Pa, Pn, cap, r2, s0 ? r2 : r2 - m0, s, mq);
+      }
     }
     if (s < m0) fin0 ^= 1;
     if (s < m1) fin1 ^= 1;
     cur ^= 1;
-    __syncthreads();
+    // Rows are owned by thread r mod 128, so a level with stride >= 128 reads
+    // and writes only the calling thread's rows: no barrier is needed before
+    // the next such level.  Earlier levels read other threads' rows, and the
+    // solve below does too, so those transitions keep the barrier.
+    if (s < kThreads || 2 * s >= mmax) __syncthreads();
   }
   // diagonal solve + end-moment recovery (M[0], M[n-1] by the owners of the end rows)
   for (int r = tid; r < mt; r += kThreads) {
@@ -529,6 +589,11 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     const double* x = s0 ? x0b : x1b;
     double Mk1 = Pf[3 * cap + r] / Pf[cap + r];
     M[k + 1] = Mk1;
+#if EMDB_FAST_DIV
+    double* R = s0 ? K.R[0] : K.R[1];
+    R[k] = 1.0 / (x[k + 1] - x[k]);
+    if (k == mq - 1) R[k + 1] = 1.0 / (x[k + 2] - x[k + 1]);
+#endif
     if (k == 0) {
       double M2 = Pf[3 * cap + r + 1] / Pf[cap + r + 1];
       double h0 = x[1] - x[0], h1 = x[2] - x[1];
@@ -543,10 +608,12 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
   __syncthreads();
 }
 
+// One PCR row update (kernels.py:651-668), in the reference's operation order.
 struct SideView {
   const double* x;
   const double* y;
   const double* M;
+  const double* R;
   int n;          // knots
   int nl, nt;     // mirrored-left and true knots
 };
@@ -569,9 +636,17 @@ __device__ __forceinline__ double eval_seg(const SideView& s, double t, int lo) 
   double y0 = y[lo], y1 = y[lo + 1];
   double M0 = s.M[lo], M1 = s.M[lo + 1];
   double h = x1 - x0;
+#if EMDB_FAST_DIV
+  double rh = s.R[lo];
+  double A = div_rn(x1 - t, h, rh);
+  double B = div_rn(t - x0, h, rh);
+  double num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
+  return (A * y0 + B * y1) + div_rn(num, 6.0, kInv6);
+#else
   double A = (x1 - t) / h;
   double B = (t - x0) / h;
   return A * y0 + B * y1 + ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h) / 6.0;
+#endif
 }
 
 // The reference's per-sample binary search (kernels.py:722-726).
@@ -654,9 +729,9 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   solve_splines(K, kb0, kb1, kn0, kn1, tid);
 
   SideView sv0, sv1;
-  sv0.x = K.X[0] + kb0; sv0.y = K.Y[0] + kb0; sv0.M = K.M[0];
+  sv0.x = K.X[0] + kb0; sv0.y = K.Y[0] + kb0; sv0.M = K.M[0]; sv0.R = K.R[0];
   sv0.n = kn0; sv0.nl = NB - kb0; sv0.nt = e.n_max;
-  sv1.x = K.X[1] + kb1; sv1.y = K.Y[1] + kb1; sv1.M = K.M[1];
+  sv1.x = K.X[1] + kb1; sv1.y = K.Y[1] + kb1; sv1.M = K.M[1]; sv1.R = K.R[1];
   sv1.n = kn1; sv1.nl = NB - kb1; sv1.nt = e.n_min;
 
   ps.sq = ps.dsq = ps.osq = ps.std_ = 0.0;
@@ -673,9 +748,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   const int wn0 = C.w_min[0], wn1 = C.w_min[1], wn2 = C.w_min[2];
   const int c1e = nch / kWarps, c2e = (2 * nch) / kWarps, c3e = (3 * nch) / kWarps;
   const unsigned incl = lane == 31 ? kFull : ((2u << lane) - 1u);
-  for (int i = tid; i < N; i += kThreads) {
-    const double t = T(i);
-    int lo0 = 0, lo1 = 0;
+  // knot segment of sample i for both envelopes
+  auto segs = [&](int i, double t, int& lo0, int& lo1) {
+    lo0 = 0;
+    lo1 = 0;
     if (fast) {
       const int c = i >> 5;
       // rank offset of the warp that scanned chunk c
@@ -689,15 +765,38 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       if (sv0.n >= 4) lo0 = search_seg(sv0, t);
       if (sv1.n >= 4) lo1 = search_seg(sv1, t);
     }
-    oor |= (t < sv0.x[0]) || (t > sv0.x[sv0.n - 1]) ||
-           (t < sv1.x[0]) || (t > sv1.x[sv1.n - 1]);
+  };
+  const double xa0 = sv0.x[0], xb0 = sv0.x[sv0.n - 1], xa1 = sv1.x[0], xb1 = sv1.x[sv1.n - 1];
+  // two samples per trip (i, i+128): independent evaluation chains overlap;
+  // each lane still accumulates its samples in increasing order
+  for (int i = tid; i < N; i += (1 + EMDB_EVAL_PAIR) * kThreads) {
+    const int i2 = i + kThreads;
+    const bool has2 = EMDB_EVAL_PAIR && i2 < N;
+    const double t = T(i);
+    const double t2 = has2 ? T(i2) : t;
+    int lo0, lo1, lo0b, lo1b;
+    segs(i, t, lo0, lo1);
+    if (has2) segs(i2, t2, lo0b, lo1b); else { lo0b = lo0; lo1b = lo1; }
+    oor |= (t < xa0) || (t > xb0) || (t < xa1) || (t > xb1);
     const double emax = eval_seg(sv0, t, lo0);
     const double emin = eval_seg(sv1, t, lo1);
-    const double mean = 0.5 * (emax + emin);
-    const double old = imf[i];
-    const double nw = old - mean;
-    imf[i] = nw;
-    accumulate(ps, old, nw);
+    const double emax2 = eval_seg(sv0, t2, lo0b);
+    const double emin2 = eval_seg(sv1, t2, lo1b);
+    {
+      const double mean = 0.5 * (emax + emin);
+      const double old = imf[i];
+      const double nw = old - mean;
+      imf[i] = nw;
+      accumulate(ps, old, nw);
+    }
+    if (has2) {
+      oor |= (t2 < xa0) || (t2 > xb0) || (t2 < xa1) || (t2 > xb1);
+      const double mean = 0.5 * (emax2 + emin2);
+      const double old = imf[i2];
+      const double nw = old - mean;
+      imf[i2] = nw;
+      accumulate(ps, old, nw);
+    }
   }
   // per-lane partial sums for the 128-lane trees
   double* red = L.red;
@@ -711,7 +810,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
 // ---------------------------------------------------------------------------
 // The sift kernel.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
+// kMinBlocks is the register-budget variant: the compiler fits the kernel
+// into 65536 / (128 * kMinBlocks) registers so that many CTAs can be resident.
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftParams p) {
   extern __shared__ __align__(16) char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int NB = p.nbsym;
@@ -760,6 +862,7 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
     bool finished = false;
     int extNo_last = -1;
     bool stale = false;
+    unsigned long long passes = 0, spilled = 0;
 
     ExtInfo e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
     ovf |= e.overflow;
@@ -781,10 +884,13 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
         }
         const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
         int flags;
-        if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes)
+        if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
           flags = sift_pass<true>(L, slab, e, N, NB, T, tid, warp, lane);
-        else
+        } else {
           flags = sift_pass<false>(L, slab, e, N, NB, T, tid, warp, lane);
+          ++spilled;
+        }
+        ++passes;
         const bool pass_bad = (flags & 1) != 0;
         stale |= (flags & 2) != 0;
         double* red = L.red;
@@ -896,6 +1002,10 @@ __global__ void __launch_bounds__(kThreads, 4) emd_sift_kernel(SiftParams p) {
     if (tid == 0) {
       p.n_imfs[b] = nim;
       p.overflow[b] = ovf ? 1 : 0;
+      if (p.counters) {
+        atomicAdd(p.counters, passes);
+        atomicAdd(p.counters + 1, spilled);
+      }
     }
     if (stale) atomicOr(p.status, kStatusStaleEnvelope);
     for (int k = tid; k < MAXI; k += kThreads) {
@@ -929,9 +1039,9 @@ __device__ __forceinline__ void envelope_pass(const SmemLayout& L, char* slab, c
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
   solve_splines(K, kb0, kb1, kn0, kn1, tid);
   SideView sv[2];
-  sv[0].x = K.X[0] + kb0; sv[0].y = K.Y[0] + kb0; sv[0].M = K.M[0]; sv[0].n = kn0;
+  sv[0].x = K.X[0] + kb0; sv[0].y = K.Y[0] + kb0; sv[0].M = K.M[0]; sv[0].R = K.R[0]; sv[0].n = kn0;
   sv[0].nl = NB - kb0; sv[0].nt = e.n_max;
-  sv[1].x = K.X[1] + kb1; sv[1].y = K.Y[1] + kb1; sv[1].M = K.M[1]; sv[1].n = kn1;
+  sv[1].x = K.X[1] + kb1; sv[1].y = K.Y[1] + kb1; sv[1].M = K.M[1]; sv[1].R = K.R[1]; sv[1].n = kn1;
   sv[1].nl = NB - kb1; sv[1].nt = e.n_min;
   nk[0] = kn0;
   nk[1] = kn1;
@@ -1018,6 +1128,64 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Self-test of div_rn against the hardware division.  mode 0: every integer
+// pair 0 <= a <= b <= n (the operands of A and B on the default time axis,
+// where knot spacings are integers <= 2N); mode 1: n pseudo-random pairs with
+// significands and exponents spread over [2^-600, 2^600] plus numerators
+// formed like the spline's h^2-scaled term over 6.  Counts mismatching bits.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__global__ void div_check_kernel(int mode, long long n, unsigned long long seed,
+                                 unsigned long long* mismatches) {
+  unsigned long long bad0 = 0, bad1 = 0, bad2 = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (mode == 0) {
+    // pairs indexed by b in [1, n]: thread grid-strides over b, loops over a
+    for (long long bb = 1 + blockIdx.x * (long long)blockDim.x + threadIdx.x; bb <= n; bb += stride) {
+      const double b = (double)bb;
+      const double y = 1.0 / b;
+      for (long long aa = 0; aa <= bb; ++aa) {
+        const double a = (double)aa;
+        if (__double_as_longlong(div_rn(a, b, y)) != __double_as_longlong(a / b)) ++bad0;
+      }
+    }
+  } else {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+      uint64_t h1 = mix64(seed ^ (uint64_t)i), h2 = mix64(h1 ^ 0x5bd1e995ull);
+      // significands in [1,2), exponents in [-300, 300] (quotients stay in range), random signs
+      double ma = __longlong_as_double((long long)((h1 >> 12) | 0x3ff0000000000000ull));
+      double mb = __longlong_as_double((long long)((h2 >> 12) | 0x3ff0000000000000ull));
+      int ea = (int)(h1 % 601) - 300, eb = (int)(h2 % 601) - 300;
+      double a = ldexp(ma, ea), b = ldexp(mb, eb);
+      if (h1 & 1) a = -a;
+      if (h2 & 2) b = -b;
+      if (__double_as_longlong(div_rn(a, b, 1.0 / b)) != __double_as_longlong(a / b)) ++bad0;
+      // division by 6 (the spline term's divisor)
+      if (__double_as_longlong(div_rn(a, 6.0, kInv6)) != __double_as_longlong(a / 6.0)) ++bad1;
+      // segment quotients: 0 <= a <= b, b a spacing in [1, 65536] with a random fraction
+      double bi = (double)((h2 >> 40) % 65536 + 1) + (double)((h2 >> 8) & 0xffff) * 0x1p-16;
+      double ai = bi * ((double)((h1 >> 11) & 0xfffffffffffffull) * 0x1p-52);
+      if (__double_as_longlong(div_rn(ai, bi, 1.0 / bi)) != __double_as_longlong(ai / bi)) ++bad2;
+    }
+  }
+  if (bad0) atomicAdd(mismatches, bad0);
+  if (bad1) atomicAdd(mismatches + 1, bad1);
+  if (bad2) atomicAdd(mismatches + 2, bad2);
+}
+
+cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
+                             unsigned long long* mismatches, cudaStream_t stream) {
+  div_check_kernel<<<148 * 8, 256, 0, stream>>>(mode, n, seed, mismatches);
+  return cudaGetLastError();
+}
+
 size_t sift_fixed_smem(int N) { return fixed_bytes(N); }
 
 size_t sift_slab_bytes(int max_extrema, int nbsym) {
@@ -1025,20 +1193,41 @@ size_t sift_slab_bytes(int max_extrema, int nbsym) {
   return align16(knot_bytes(kc, kc));
 }
 
-cudaError_t sift_occupancy(int arena_bytes, int* ctas_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+namespace {
+template <int V>
+cudaError_t occupancy_v(int arena_bytes, int* ctas_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        arena_bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_sift_kernel, kThreads,
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_sift_kernel<V>, kThreads,
                                                        arena_bytes);
+}
+template <int V>
+cudaError_t launch_v(const SiftParams& p, int grid, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       p.arena_bytes);
+  if (e != cudaSuccess) return e;
+  emd_sift_kernel<V><<<grid, kThreads, p.arena_bytes, stream>>>(p);
+  return cudaGetLastError();
+}
+}  // namespace
+
+bool sift_variant_ok(int v) { return v == 4 || v == 5 || v == 6; }
+
+cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm) {
+  switch (variant) {
+    case 5: return occupancy_v<5>(arena_bytes, ctas_per_sm);
+    case 6: return occupancy_v<6>(arena_bytes, ctas_per_sm);
+    default: return occupancy_v<4>(arena_bytes, ctas_per_sm);
+  }
 }
 
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       p.arena_bytes);
-  if (e != cudaSuccess) return e;
-  emd_sift_kernel<<<grid, kThreads, p.arena_bytes, stream>>>(p);
-  return cudaGetLastError();
+  switch (p.variant) {
+    case 5: return launch_v<5>(p, grid, stream);
+    case 6: return launch_v<6>(p, grid, stream);
+    default: return launch_v<4>(p, grid, stream);
+  }
 }
 
 cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm) {

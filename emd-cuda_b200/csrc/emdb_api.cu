@@ -18,7 +18,9 @@ struct emdb_plan {
   int num_sms = 0;
   int smem_optin = 0;
   int arena_override = 0;
+  int variant = 4;            // register-budget variant (min CTAs per SM)
   int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
+  unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes
   char* d_slab = nullptr;
   size_t slab_stride = 0;
   int slab_ctas = 0;
@@ -59,7 +61,7 @@ int auto_arena(const emdb_plan* p, int max_n) {
   const int per_sm = 233472;
   size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
   int best = 0;
-  for (int want = 4; want >= 1; --want) {
+  for (int want = p->variant; want >= 1; --want) {
     int arena = per_sm / want - 1024;
     arena = std::min(arena, p->smem_optin);
     arena &= ~15;
@@ -113,14 +115,16 @@ int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st
     return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
                 " does not fit this device's shared memory");
   int per_sm = 0;
-  cudaError_t e = emdb::sift_occupancy(arena, &per_sm);
+  cudaError_t e = emdb::sift_occupancy(arena, p->variant, &per_sm);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
   int grid = std::min(sp.batch, per_sm * p->num_sms);
+  sp.variant = p->variant;
   int rc = ensure_slab(p, grid);
   if (rc) return rc;
   sp.queue = p->d_ctl;
   sp.status = p->d_ctl + 1;
+  sp.counters = p->d_cnt;
   sp.slab = p->d_slab;
   sp.slab_stride = p->slab_stride;
   sp.arena_bytes = arena;
@@ -171,6 +175,13 @@ int emdb_plan_create(const emdb_config* cfg, int device, emdb_plan** out) {
     return cuda_fail(e, "allocating plan control words");
   }
   cudaMemset(p->d_ctl, 0, 4 * sizeof(int));
+  e = cudaMalloc(&p->d_cnt, 2 * sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    cudaFree(p->d_ctl);
+    delete p;
+    return cuda_fail(e, "allocating plan counters");
+  }
+  cudaMemset(p->d_cnt, 0, 2 * sizeof(unsigned long long));
   *out = p;
   return EMDB_OK;
 }
@@ -181,6 +192,7 @@ int emdb_plan_destroy(emdb_plan* p) {
     DeviceGuard g(p->device);
     if (p->d_slab) cudaFree(p->d_slab);
     if (p->d_ctl) cudaFree(p->d_ctl);
+    if (p->d_cnt) cudaFree(p->d_cnt);
   }
   delete p;
   return EMDB_OK;
@@ -195,13 +207,22 @@ int emdb_plan_set_arena(emdb_plan* p, int arena_bytes) {
   return EMDB_OK;
 }
 
+int emdb_plan_set_variant(emdb_plan* p, int min_ctas_per_sm) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (!emdb::sift_variant_ok(min_ctas_per_sm))
+    return fail(EMDB_ERR_INVALID, "variant must be 4, 5 or 6 CTAs per SM");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->variant = min_ctas_per_sm;
+  return EMDB_OK;
+}
+
 int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm, int* grid_max) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   DeviceGuard g(p->device);
   int arena = arena_for(p, max_n);
   int per_sm = 0;
   if (arena > 0) {
-    cudaError_t e = emdb::sift_occupancy(arena, &per_sm);
+    cudaError_t e = emdb::sift_occupancy(arena, p->variant, &per_sm);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   }
   if (arena_bytes) *arena_bytes = arena;
@@ -316,6 +337,37 @@ int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batc
   if (e != cudaSuccess) return cuda_fail(e, "queue reset");
   e = emdb::launch_envelope(ep, grid, st);
   if (e != cudaSuccess) return cuda_fail(e, "envelope launch");
+  return EMDB_OK;
+}
+
+int emdb_plan_counters(emdb_plan* p, unsigned long long* passes, unsigned long long* spilled,
+                       int reset) {
+  if (!p || !passes || !spilled) return fail(EMDB_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(h, p->d_cnt, sizeof(h), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && reset) e = cudaMemset(p->d_cnt, 0, sizeof(h));
+  if (e != cudaSuccess) return cuda_fail(e, "counter read-back");
+  *passes = h[0];
+  *spilled = h[1];
+  return EMDB_OK;
+}
+
+int emdb_check_division(int mode, long long n, unsigned long long seed,
+                        unsigned long long* mismatches) {
+  if (!mismatches || (mode != 0 && mode != 1) || n < 0)
+    return fail(EMDB_ERR_INVALID, "bad self-test arguments");
+  unsigned long long* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, 3 * sizeof(unsigned long long));
+  if (e != cudaSuccess) return cuda_fail(e, "self-test counter");
+  e = cudaMemset(d, 0, 3 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = emdb::launch_div_check(mode, n, seed, d, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(mismatches, d, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return cuda_fail(e, "division self-test");
   return EMDB_OK;
 }
 

@@ -39,6 +39,7 @@ struct SiftParams {
   // scratch
   int* queue;                 // work-queue ticket counter (zeroed before launch)
   int* status;                // error word (OR of kStatus*)
+  unsigned long long* counters;  // [0] sift passes, [1] passes on the global slab (may be NULL)
   char* slab;                 // per-CTA global spill area
   size_t slab_stride;         // bytes per CTA
   int arena_bytes;            // dynamic shared memory per CTA
@@ -47,6 +48,7 @@ struct SiftParams {
   int nbsym;
   int max_iteration;
   int max_imfs;
+  int variant;                // register-budget variant: min CTAs per SM (4, 5, 6)
 };
 
 struct EnvParams {
@@ -82,7 +84,10 @@ size_t sift_slab_bytes(int max_extrema, int nbsym);
 
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream);
 cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream);
-cudaError_t sift_occupancy(int arena_bytes, int* ctas_per_sm);
+bool sift_variant_ok(int variant);
+cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm);
 cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm);
+cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
+                             unsigned long long* mismatches, cudaStream_t stream);
 
 }  // namespace emdb

@@ -24,9 +24,11 @@ STATUS_TOO_LONG = 2
 
 # Every symbol include/emdb200.h declares (checked by the CPU test suite).
 EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_set_arena",
+           "emdb_plan_set_variant",
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
-           "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16")
+           "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
+           "emdb_plan_counters")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -57,12 +59,16 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_create.argtypes = [ctypes.POINTER(EmdbConfig), I, ctypes.POINTER(VP)]
         L.emdb_plan_destroy.argtypes = [VP]
         L.emdb_plan_set_arena.argtypes = [VP, I]
+        L.emdb_plan_set_variant.argtypes = [VP, I]
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_ragged.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]
         L.emdb_envelope.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
         L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
         L.emdb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        L.emdb_plan_counters.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
+                                         ctypes.POINTER(ctypes.c_ulonglong), I]
+        L.emdb_check_division.argtypes = [I, ctypes.c_longlong, ctypes.c_ulonglong, P]
         for name in EXPORTS:
             getattr(L, name).restype = I
         _lib = L
@@ -118,13 +124,32 @@ class Plan:
     def set_arena(self, arena_bytes: int) -> None:
         check(self.L.emdb_plan_set_arena(self.handle, int(arena_bytes)), "emdb_plan_set_arena")
 
+    def set_variant(self, min_ctas_per_sm: int) -> None:
+        check(self.L.emdb_plan_set_variant(self.handle, int(min_ctas_per_sm)), "emdb_plan_set_variant")
+
     def query(self, max_n: int) -> tuple[int, int, int]:
         a, c, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(self.L.emdb_plan_query(self.handle, int(max_n), ctypes.byref(a), ctypes.byref(c),
                                      ctypes.byref(g)), "emdb_plan_query")
         return a.value, c.value, g.value
 
+    def counters(self, reset: bool = False) -> tuple[int, int]:
+        """(sift passes, passes spilled to the global slab) since creation / last reset."""
+        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        check(self.L.emdb_plan_counters(self.handle, ctypes.byref(a), ctypes.byref(b), int(reset)),
+              "emdb_plan_counters")
+        return a.value, b.value
+
     def status(self, stream: int) -> int:
         s = ctypes.c_int()
         check(self.L.emdb_status(self.handle, ctypes.byref(s), ctypes.c_void_p(stream)), "emdb_status")
         return s.value
+
+
+def check_division(mode: int, n: int, seed: int = 0) -> tuple[int, int, int]:
+    """Mismatches of the reciprocal-based division vs the hardware division,
+    per case: (general a/b, a/6, segment quotients).  Self-test."""
+    L = load()
+    out = (ctypes.c_ulonglong * 3)()
+    check(L.emdb_check_division(int(mode), int(n), int(seed), out), "emdb_check_division")
+    return tuple(int(v) for v in out)

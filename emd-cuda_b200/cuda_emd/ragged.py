@@ -13,9 +13,10 @@ be captured once into a CUDA graph and replayed.
 Queue order inside a tier is FIFO (trace index) or, given per-trace costs,
 longest-predicted-first.  Order never changes a result.
 
-The autotuner times every candidate arena (1..4 CTAs per SM, plus the
-minimum that fits) on a sample of each tier and caches the winner in a JSON
-file keyed by device, config and tier.
+The autotuner times every candidate (register-budget variant, arena) pair --
+the largest arena that keeps k = 6..1 CTAs per SM resident, with the kernel
+build compiled for max(k, 4) CTAs -- on a sample of each tier and caches the
+winner in a JSON file keyed by device, config and tier.
 """
 from __future__ import annotations
 
@@ -40,20 +41,21 @@ def tier_of(n: int) -> int:
     raise ValueError(f"trace length {n} exceeds the largest tier {TIER_EDGES[-1]}")
 
 
-def candidate_arenas(plan: _native.Plan, max_n: int) -> list[int]:
-    """Arena sizes worth trying for traces up to max_n: the largest arena
-    that keeps k CTAs per SM resident, k = 4..1, if it holds the trace."""
-    auto, _, _ = plan.query(max_n)
-    fixed_min = auto if auto > 0 else 0
+def candidates(plan: _native.Plan, max_n: int) -> list[tuple[int, int]]:
+    """(register variant, arena) pairs worth trying for traces up to max_n:
+    the largest arena that keeps k CTAs per SM resident, k = 6..1, with the
+    register-budget build for max(k, 4) CTAs, if the arena holds the trace."""
+    plan.set_variant(4)
+    plan.set_arena(0)
+    auto, _, _ = plan.query(max_n)            # smallest arena that holds a trace
     out = []
-    for k in (4, 3, 2, 1):
-        a = (SMEM_PER_SM // k - CTA_RESERVED) & ~15
-        a = min(a, 232448)
-        if a >= fixed_min or (auto > 0 and a >= auto):
-            out.append(a)
-    if auto > 0 and auto not in out:
-        out.append(auto)
-    return sorted(set(out))
+    for k in (6, 5, 4, 3, 2, 1):
+        a = min((SMEM_PER_SM // k - CTA_RESERVED) & ~15, 232448)
+        if auto > 0 and a >= auto:
+            out.append((max(k, 4), a))
+    if not out and auto > 0:
+        out.append((4, auto))
+    return out
 
 
 class Tier:
@@ -63,9 +65,12 @@ class Tier:
         self.max_n = 0
         self.plan = _native.Plan(cfg.to_c(), device)
         self.arena = 0
+        self.variant = 4
 
-    def set_arena(self, a: int) -> None:
-        self.arena = int(a)
+    def set_tuning(self, variant: int, arena: int) -> None:
+        self.variant = int(variant)
+        self.arena = int(arena)
+        self.plan.set_variant(self.variant)
         self.plan.set_arena(self.arena)
 
 
@@ -129,21 +134,23 @@ class RaggedRunner:
         for t in tiers:
             key = self._key(t.edge)
             if key in self._cache:
-                t.set_arena(self._cache[key]["arena"])
-                chosen[t.edge] = self._cache[key]
+                c = self._cache[key]
+                t.set_tuning(c.get("variant", 4), c["arena"])
+                chosen[t.edge] = c
                 continue
-            cands = candidate_arenas(t.plan, t.edge)
+            cands = candidates(t.plan, t.edge)
             if not cands:
                 raise ValueError(f"tier {t.edge} does not fit this device")
             if len(cands) == 1 or not self.autotune:
-                t.set_arena(cands[-1] if not self.autotune else cands[0])
+                v4 = [c for c in cands if c[0] == 4]
+                t.set_tuning(*(v4[0] if v4 else cands[0]))
                 continue
-            n_s = sample or min(t.idx.size, 4 * 148 * 4)
+            n_s = sample or min(t.idx.size, 6 * 148 * 3)
             sub = torch.from_numpy(t.idx[:n_s].astype(np.int32)).to(values.device)
             res = {}
-            for a in cands:
-                t.set_arena(a)
-                outs = self._alloc_out(values, offsets)
+            outs = self._alloc_out(values, offsets)
+            for v, a in cands:
+                t.set_tuning(v, a)
                 self._launch_tier(t, values, offsets, sub, outs)       # warm
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -151,11 +158,12 @@ class RaggedRunner:
                 self._launch_tier(t, values, offsets, sub, outs)
                 e1.record()
                 e1.synchronize()
-                res[a] = e0.elapsed_time(e1)
-                del outs
+                res[(v, a)] = e0.elapsed_time(e1)
+            del outs
             best = min(res, key=res.get)
-            t.set_arena(best)
-            self._cache[key] = {"arena": best, "ms": res[best], "tried": {str(k): v for k, v in res.items()},
+            t.set_tuning(*best)
+            self._cache[key] = {"variant": best[0], "arena": best[1], "ms": res[best],
+                                "tried": {f"{v}/{a}": ms for (v, a), ms in res.items()},
                                 "sample": int(n_s)}
             chosen[t.edge] = self._cache[key]
         self._save_cache()
@@ -183,7 +191,19 @@ class RaggedRunner:
             dn.data_ptr(), de.data_ptr(), dz.data_ptr(), st), "emdb_run_ragged")
 
     def prepare(self, values, offsets, cost=None):
-        """Host-side plan: tiers and per-tier queue orders (device int32)."""
+        """Host-side plan: tiers and per-tier queue orders (device int32).
+        Cached for repeated calls on the same offsets / cost tensors."""
+        import torch
+        key = (offsets.data_ptr(), int(offsets.shape[0]), values.data_ptr(),
+               None if cost is None else cost.data_ptr())
+        cached = getattr(self, "_prep", None)
+        if cached is not None and cached[0] == key:
+            return cached[1], cached[2]
+        tiers, orders = self._prepare(values, offsets, cost)
+        self._prep = (key, tiers, orders)
+        return tiers, orders
+
+    def _prepare(self, values, offsets, cost=None):
         import torch
         off_h = offsets.cpu().numpy() if hasattr(offsets, "cpu") else np.asarray(offsets)
         lengths = np.diff(off_h)

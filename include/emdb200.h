@@ -66,6 +66,10 @@ int emdb_plan_destroy(emdb_plan* plan);
  * autotuner sets this; larger arenas spill fewer knots but fit fewer CTAs
  * per SM.  Fails if the arena cannot hold a trace of length max_n. */
 int emdb_plan_set_arena(emdb_plan* plan, int arena_bytes);
+/* Register-budget variant of the sift kernel: the kernel instance compiled
+ * for at least `min_ctas_per_sm` (4, 5 or 6) resident 128-thread CTAs per SM;
+ * the automatic arena then targets that many CTAs.  Chosen by the autotuner. */
+int emdb_plan_set_variant(emdb_plan* plan, int min_ctas_per_sm);
 /* Arena and CTAs/SM the plan would use for traces up to max_n. */
 int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
                     int* grid_max);
@@ -101,6 +105,12 @@ int emdb_envelope(emdb_plan* plan, const double* signals, const double* T, int b
                   double* max_env, double* min_env, int* n_extrema, int* degenerate,
                   double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
                   int* n_mirrored, void* stream);
+
+/* Sift passes the plan's launches have run so far, and how many of them kept
+ * their knots in the global spill slab instead of shared memory (tuning
+ * diagnostics).  Synchronises the device; reset != 0 clears the counters. */
+int emdb_plan_counters(emdb_plan* plan, unsigned long long* passes,
+                       unsigned long long* spilled, int reset);
 
 /* Synchronise `stream`, read and clear the plan's device status word
  * (EMDB_STATUS_* bits) into *status. */
@@ -139,6 +149,15 @@ int emdb_mlp_adam(float* params, const float* grads, float* m, float* v, int n, 
 /* Inference with bfloat16 weights and FP32 accumulation: Y [B,2]. */
 int emdb_mlp_infer_bf16(const uint16_t* params_bf16, const float* X, const float* mu,
                         const float* sd, int B, float* Y, void* stream);
+
+/* Self-test of the division the kernels use where a reciprocal is at hand
+ * (no reference counterpart): counts results that differ in any bit from the
+ * hardware IEEE division, in mismatches[3] (host array).  mode 0: every
+ * integer pair 0 <= a <= b <= n (count in [0]); mode 1: n seeded random
+ * cases each of [0] a/b over [2^-300, 2^300], [1] a/6, [2] a/b with
+ * 0 <= a <= b, b in [1, 65537).  Synchronous on the current device. */
+int emdb_check_division(int mode, long long n, unsigned long long seed,
+                        unsigned long long* mismatches);
 
 /* Message of the calling thread's last error ("" if none). */
 int emdb_last_error(char* buf, size_t len);

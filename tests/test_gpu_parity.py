@@ -223,3 +223,29 @@ def test_arena_too_small_raises():
     L._plan.set_arena(20000)
     with pytest.raises(ValueError):
         L.run(torch.zeros((2, 2048), dtype=torch.float64, device="cuda"), None)
+
+
+@pytest.mark.parametrize("variant", [5, 6])
+def test_register_variants_same_results(variant):
+    """The 5- and 6-CTA/SM register-budget builds compute the same bits."""
+    import torch
+    from cuda_emd import EMDKernelConfig, workloads as W
+    X = torch.from_numpy(W.seismic_batch(40, 2048, seed=400)).cuda()
+    L = EMDKernelConfig().build()
+    ref = [o.cpu() for o in L.run(X, None)]
+    L._plan.set_variant(variant)
+    out = [o.cpu() for o in L.run(X, None)]
+    L.check_status()
+    for a, b in zip(ref, out):
+        assert torch.equal(a, b)
+
+
+def test_division_matches_hardware():
+    """The reciprocal-based division used in envelope evaluation equals the
+    IEEE division bit for bit: exhaustively over every integer pair
+    0 <= a <= b <= 65536 (all A/B operands on the default time axis for traces
+    up to 32768 samples) and on 4e8 pseudo-random pairs."""
+    from cuda_emd import _native
+    assert _native.check_division(0, 65536) == (0, 0, 0)
+    for seed in range(4):
+        assert _native.check_division(1, 100_000_000, seed=seed) == (0, 0, 0)
