@@ -27,6 +27,7 @@ UNITS = [
     ("emd_sift.cu", ["-fmad=false"]),
     ("emd_sched.cu", []),
     ("emdb_api.cu", []),
+    ("emdb_noalloc.cu", []),
 ]
 HEADERS = ["emdb_internal.cuh", "emdb_sched.cuh"]
 

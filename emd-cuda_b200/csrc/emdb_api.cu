@@ -355,6 +355,11 @@ int emdb_plan_counters(emdb_plan* p, unsigned long long* passes, unsigned long l
   return EMDB_OK;
 }
 
+// Error reporting hook for the no-allocation entry point (emdb_noalloc.cu).
+__attribute__((visibility("hidden"))) int emdb_noalloc_fail(int code, const char* msg) {
+  return fail(code, msg);
+}
+
 int emdb_check_division(int mode, long long n, unsigned long long seed,
                         unsigned long long* mismatches) {
   if (!mismatches || (mode != 0 && mode != 1) || n < 0)

@@ -28,7 +28,7 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
-           "emdb_plan_counters")
+           "emdb_plan_counters", "emdb_run_noalloc")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -66,6 +66,7 @@ def load() -> ctypes.CDLL:
         L.emdb_envelope.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
         L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
         L.emdb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+        L.emdb_run_noalloc.argtypes = [ctypes.POINTER(EmdbConfig), P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_plan_counters.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong), I]
         L.emdb_check_division.argtypes = [I, ctypes.c_longlong, ctypes.c_ulonglong, P]

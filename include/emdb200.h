@@ -112,6 +112,24 @@ int emdb_envelope(emdb_plan* plan, const double* signals, const double* T, int b
 int emdb_plan_counters(emdb_plan* plan, unsigned long long* passes,
                        unsigned long long* spilled, int reset);
 
+/* Dense batch like emdb_run, for callers that cannot allocate device memory:
+ * code running under CUDA stream capture (allocation is illegal there),
+ * services that reserve all device memory up front and forbid allocations on
+ * the request path, hosts whose own allocator owns the device.  No plan is
+ * needed: the scratch (work-queue ticket, status word, per-CTA spill slab) is
+ * one 32 MiB file-scope device array, held by every GPU that loads the
+ * library until the process exits.  The slab bounds how many CTAs a call
+ * runs; a config whose per-CTA slab does not fit the array even once is
+ * rejected with EMDB_ERR_UNSUPPORTED.  Runs on the current device,
+ * asynchronously on `stream`; the device status word is not reported (check
+ * `overflow`; T must already be validated).  Every call shares the array:
+ * calls that overlap on the GPU race, so serialise them.  A device's first
+ * call looks up the array's address; make it outside any stream capture.
+ * No counterpart in the reference (its run() always allocates, kernels.py:1353-1363). */
+int emdb_run_noalloc(const emdb_config* cfg, const double* signals, const double* T, int batch,
+                     int N, double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                     int* dbg_nzm, void* stream);
+
 /* Synchronise `stream`, read and clear the plan's device status word
  * (EMDB_STATUS_* bits) into *status. */
 int emdb_status(emdb_plan* plan, int* status, void* stream);
