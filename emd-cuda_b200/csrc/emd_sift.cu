@@ -322,6 +322,14 @@ __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots
   for (int c = c0; c < c1; ++c) {
     uint32_t bm = L.mmax[c], bn = L.mmin[c];
     bool ismax = (bm >> lane) & 1u, ismin = (bn >> lane) & 1u;
+    // after the ranks below are taken, the chunk's prefix becomes global
+    // (warp offset added) for the evaluation pass's segment counts
+    const int pm = L.pmax[c], pn = L.pmin[c];
+    __syncwarp();
+    if (lane == 0) {
+      L.pmax[c] = (uint16_t)(pm + e.off_max);
+      L.pmin[c] = (uint16_t)(pn + e.off_min);
+    }
     if (!(ismax || ismin)) continue;
     int i = (c << 5) + lane;
     int ii = i;
@@ -336,8 +344,8 @@ __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots
       }
     }
     int q = ismax ? 0 : 1;
-    int rank = q == 0 ? e.off_max + L.pmax[c] + __popc(bm & lt)
-                      : e.off_min + L.pmin[c] + __popc(bn & lt);
+    int rank = q == 0 ? e.off_max + pm + __popc(bm & lt)
+                      : e.off_min + pn + __popc(bn & lt);
     int nq = q == 0 ? e.n_max : e.n_min;
     if (rank < nq) {
       double* Xq = q == 0 ? K.X[0] : K.X[1];
@@ -659,19 +667,6 @@ __device__ __forceinline__ int search_seg(const SideView& s, double t) {
   return lo;
 }
 
-// Same answer in O(1) for a strictly increasing knot list: the number of knots
-// at or left of t, less one, where the true knots are counted from the last
-// extrema scan's ballot masks (prefix per chunk + popc within the chunk).
-__device__ __forceinline__ int count_seg(const SideView& s, double t, int cnt_true) {
-  int k = min(cnt_true, s.nt);
-  for (int j = 0; j < s.nl; ++j) k += s.x[j] <= t;
-  const double* xr = s.x + s.nl + s.nt;
-  for (int j = 0; j < s.n - s.nl - s.nt; ++j) k += xr[j] <= t;
-  int lo = k - 1;
-  lo = lo < 0 ? 0 : lo;
-  return lo > s.n - 2 ? s.n - 2 : lo;
-}
-
 // 128-lane tree of the reference (kernels.py:794-804), on warp 0, for a value
 // each thread has stored at red[q*128 + tid].  op 0: sum, 1: fmax, 2: fmin.
 __device__ __forceinline__ double lane_tree(const double* red, int lane, int op) {
@@ -738,35 +733,47 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   ps.omax = -1e30;
   ps.omin = 1e30;
   bool oor = false;
-  // O(1) segments need a strictly increasing knot list: true for nbsym <= 2
-  // without flat runs (plateau extrema sit at a run midpoint, not at the
-  // flagged sample).  Otherwise use the reference's binary search.
+  // O(1) segments: for a strictly increasing knot list (nbsym <= 2, no flat
+  // runs -- a plateau extremum sits at the run's midpoint, not at its flagged
+  // first sample) the reference's binary search returns (number of knots at
+  // or left of t) - 1, clamped to [0, n-2].  Otherwise run the search.
   const bool fast = NB <= 2 && !e.trig;
   const int nch = (N + 31) >> 5;
   // chunk c = (tid>>5) + 4j is scanned by warp wc(c); its rank offset is woff[wc] + pre[c]
-  const int wm0 = C.w_max[0], wm1 = C.w_max[1], wm2 = C.w_max[2];
-  const int wn0 = C.w_min[0], wn1 = C.w_min[1], wn2 = C.w_min[2];
-  const int c1e = nch / kWarps, c2e = (2 * nch) / kWarps, c3e = (3 * nch) / kWarps;
+  // mirrored knots of both envelopes, for the O(1) segment count (nbsym <= 2)
+  constexpr double kInf = __builtin_huge_val();
+  const double l00 = sv0.nl > 0 ? sv0.x[0] : kInf, l01 = sv0.nl > 1 ? sv0.x[1] : kInf;
+  const double l10 = sv1.nl > 0 ? sv1.x[0] : kInf, l11 = sv1.nl > 1 ? sv1.x[1] : kInf;
+  const int nr0 = sv0.n - sv0.nl - sv0.nt, nr1 = sv1.n - sv1.nl - sv1.nt;
+  const double r00 = nr0 > 0 ? sv0.x[sv0.nl + sv0.nt] : kInf, r01 = nr0 > 1 ? sv0.x[sv0.nl + sv0.nt + 1] : kInf;
+  const double r10 = nr1 > 0 ? sv1.x[sv1.nl + sv1.nt] : kInf, r11 = nr1 > 1 ? sv1.x[sv1.nl + sv1.nt + 1] : kInf;
+  (void)nch;
   const unsigned incl = lane == 31 ? kFull : ((2u << lane) - 1u);
   // knot segment of sample i for both envelopes
   auto segs = [&](int i, double t, int& lo0, int& lo1) {
     lo0 = 0;
     lo1 = 0;
     if (fast) {
+      // knots at or left of t: mirrored ones compared directly, true ones
+      // counted from the scan's ballot masks (global chunk prefix + popc)
       const int c = i >> 5;
-      // rank offset of the warp that scanned chunk c
-      const int o0 = (c >= c1e ? wm0 : 0) + (c >= c2e ? wm1 : 0) + (c >= c3e ? wm2 : 0);
-      const int o1 = (c >= c1e ? wn0 : 0) + (c >= c2e ? wn1 : 0) + (c >= c3e ? wn2 : 0);
-      const int ct0 = o0 + L.pmax[c] + __popc(L.mmax[c] & incl);
-      const int ct1 = o1 + L.pmin[c] + __popc(L.mmin[c] & incl);
-      if (sv0.n >= 4) lo0 = count_seg(sv0, t, ct0);
-      if (sv1.n >= 4) lo1 = count_seg(sv1, t, ct1);
+      int k0 = min((int)L.pmax[c] + __popc(L.mmax[c] & incl), sv0.nt);
+      int k1 = min((int)L.pmin[c] + __popc(L.mmin[c] & incl), sv1.nt);
+      k0 += (l00 <= t) + (l01 <= t) + (r00 <= t) + (r01 <= t);
+      k1 += (l10 <= t) + (l11 <= t) + (r10 <= t) + (r11 <= t);
+      lo0 = min(max(k0 - 1, 0), sv0.n - 2);
+      lo1 = min(max(k1 - 1, 0), sv1.n - 2);
     } else {
       if (sv0.n >= 4) lo0 = search_seg(sv0, t);
       if (sv1.n >= 4) lo1 = search_seg(sv1, t);
     }
   };
-  const double xa0 = sv0.x[0], xb0 = sv0.x[sv0.n - 1], xa1 = sv1.x[0], xb1 = sv1.x[sv1.n - 1];
+  // T is strictly increasing, so the knot spans cover every sample iff they
+  // cover the first and the last one
+  if (N > 0) {
+    const double t0 = T(0), tN = T(N - 1);
+    oor = (t0 < sv0.x[0]) || (tN > sv0.x[sv0.n - 1]) || (t0 < sv1.x[0]) || (tN > sv1.x[sv1.n - 1]);
+  }
   // two samples per trip (i, i+128): independent evaluation chains overlap;
   // each lane still accumulates its samples in increasing order
   for (int i = tid; i < N; i += (1 + EMDB_EVAL_PAIR) * kThreads) {
@@ -777,7 +784,6 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     int lo0, lo1, lo0b, lo1b;
     segs(i, t, lo0, lo1);
     if (has2) segs(i2, t2, lo0b, lo1b); else { lo0b = lo0; lo1b = lo1; }
-    oor |= (t < xa0) || (t > xb0) || (t < xa1) || (t > xb1);
     const double emax = eval_seg(sv0, t, lo0);
     const double emin = eval_seg(sv1, t, lo1);
     const double emax2 = eval_seg(sv0, t2, lo0b);
@@ -790,7 +796,6 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       accumulate(ps, old, nw);
     }
     if (has2) {
-      oor |= (t2 < xa0) || (t2 > xb0) || (t2 < xa1) || (t2 > xb1);
       const double mean = 0.5 * (emax2 + emin2);
       const double old = imf[i2];
       const double nw = old - mean;
