@@ -39,10 +39,19 @@ sys.path.insert(0, os.path.join(ROOT, "emd-cuda_b200"))
 sys.path.insert(0, ROOT)
 
 METRIC = "EMD signals/s (FP64)"
+# DRAM bytes per trace of emd_sift_kernel, keyed by (N, max_imfs): one ncu
+# capture of the seismic1k launch (1024 traces x 2048 samples) read
+# dram__bytes_read.sum 27.14 MB + dram__bytes_write.sum 280.78 MB.  Inputs and
+# outputs are per trace and the spill slab stays in L2, so a launch's traffic
+# is this figure times its traces.
+NCU_DRAM_BYTES_PER_TRACE = {(2048, 16): 307917568 / 1024}
 WORKLOADS = {
     "seismic16k": dict(n=16384, N=2048, desc="16384 seismic traces x 2048 samples, dt 2 ms"),
     "sinusoid256": dict(n=256, N=1024, desc="256 three-tone traces x 1024 samples"),
     "seismic1k": dict(n=1024, N=2048, desc="1024 seismic traces x 2048 samples (profiling size)"),
+    "serve": dict(lo=512, hi=16384, max_traces=64,
+                  desc="Poisson requests of 1-64 traces, N log-uniform [512, 16384], ragged mix; "
+                       "offered load 10-110% of measured saturation"),
     "ragged64k": dict(n=65536, lo=256, hi=8192,
                       desc="65536 mixed traces, N log-uniform [256, 8192] (60% seismic, 38% "
                            "three-tone, 2% chirp), CSR; plain FIFO vs learned longest-first"),
@@ -178,6 +187,8 @@ def main():
     ap.add_argument("--train-traces", type=int, default=200000, help="ragged64k: MLP training set")
     ap.add_argument("--eval-traces", type=int, default=0, help="ragged64k: batch size (0 = 65536)")
     ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--requests", type=int, default=160, help="serve: requests per load level")
+    ap.add_argument("--loads", default="0.1,0.3,0.5,0.7,0.9,1.1", help="serve: offered loads")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -197,6 +208,9 @@ def main():
         return
     if a.workload == "ragged64k":
         run_ragged(a, rank, world, pool, cores)
+        return
+    if a.workload == "serve":
+        run_serve(a, rank, world, pool, cores)
         return
 
     import torch
@@ -316,8 +330,12 @@ def main():
         achieved = flops_per_step / launch_s / 1e12
         hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
         hbm_ach = hbm_bytes_per_step / launch_s / 1e9
+        per_trace = NCU_DRAM_BYTES_PER_TRACE.get((N, cfg.max_imfs))
+        traffic = round(per_trace * B) if per_trace else None
         roofline = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64, 3),
-                    "unit": "TFLOP/s", "frac": round(achieved / fp64, 4), "traffic": None,
+                    "unit": "TFLOP/s", "frac": round(achieved / fp64, 4), "traffic": traffic,
+                    "traffic_source": ("ncu dram__bytes_read+write per trace of a 1024-trace "
+                                       "launch x traces per launch") if traffic else None,
                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
                     "kernel": "emd_sift_kernel",
                     "algorithmic_flop_per_launch": flops_per_step,
@@ -590,6 +608,75 @@ def run_ragged(a, rank, world, pool, cores):
                        "mae_log2_passes": round(mae_log2_passes, 4),
                        "mae_passes": round(mae_passes, 2), "mae_n_imfs": round(mae_nimfs, 4)},
         "gen_s": round(gen_s, 1), "gpu_launches": a.steps * len(tiers),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Serving: continuous batching under Poisson load
+# ---------------------------------------------------------------------------
+
+def _gen_requests_chunk(args):
+    n, lo, hi, mt, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "emd-cuda_b200"))
+    from cuda_emd.serving import make_requests
+    rng = np.random.default_rng(seed)
+    return [r.traces for r in make_requests(n, rng, lo=lo, hi=hi, max_traces=mt)]
+
+
+def run_serve(a, rank, world, pool, cores):
+    import torch
+    from cuda_emd import EMDKernelConfig
+    from cuda_emd import scheduler as S
+    from cuda_emd.serving import EMDServer, Request, run_open_loop, poisson_arrivals
+    w = WORKLOADS["serve"]
+    nreq = a.requests
+    t0 = time.perf_counter()
+    parts = [(max(1, nreq // 8), w["lo"], w["hi"], w["max_traces"], 4000 + k) for k in range(8)]
+    res = pool.map(_gen_requests_chunk, parts) if pool is not None else [_gen_requests_chunk(p) for p in parts]
+    traces = [t for chunk in res for t in chunk][:nreq]
+    gen_s = time.perf_counter() - t0
+    if pool is not None:
+        pool.close()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    cfg = EMDKernelConfig.for_device(local)
+    # cost model for the in-batch order, trained on the plain method's counts of a small set
+    from cuda_emd.workloads import ragged_mix
+    tv, to, _ = ragged_mix(4096, lo=w["lo"], hi=4096, seed=4999)
+    tvd, tod = torch.from_numpy(tv).cuda(), torch.from_numpy(to).cuda()
+    L = cfg.build()
+    out = L.run_ragged(tvd, tod)
+    cm = S.CostModel(local, seed=0)
+    cm.fit(S.features(tvd, tod), S.labels_from_debug(out[3], out[1]), epochs=a.epochs, batch=1024)
+    del out, tvd, tod
+    mk = lambda: [Request(i, trs) for i, trs in enumerate(traces)]
+    # warm-up (plans, autotune-free tiers, kernels) and saturation (everything at t=0)
+    srv = EMDServer(cfg, local, slots=4, cost_model=cm)
+    run_open_loop(srv, mk()[:8], np.zeros(8))
+    sat = run_open_loop(EMDServer(cfg, local, slots=4, cost_model=cm), mk(), np.zeros(nreq))
+    sat_tps = sat["traces_per_s"]
+    mean_tr = sum(len(t) for t in traces) / nreq
+    rng = np.random.default_rng(77)
+    levels = []
+    for load in [float(x) for x in a.loads.split(",")]:
+        rate = load * sat_tps / mean_tr
+        arr = poisson_arrivals(rate, nreq, rng)
+        arr -= arr[0]
+        rep = run_open_loop(EMDServer(cfg, local, slots=4, cost_model=cm), mk(), arr, timeout_s=900)
+        rep.update({"offered_load": load, "offered_traces_per_s": round(load * sat_tps, 1)})
+        levels.append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in rep.items()})
+    p99_90 = next((l["p99_ms"] for l in levels if abs(l["offered_load"] - 0.9) < 1e-6), None)
+    line = {
+        "metric": "EMD serve latency (FP64)", "value": p99_90, "unit": "ms p99 at 90% load",
+        "n_gpus": world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": "serve", "desc": w["desc"], "requests_per_level": nreq,
+                   "mean_traces_per_request": round(mean_tr, 2), "slots": 4,
+                   "order": "learned longest-predicted-first inside each admitted batch"},
+        "saturation": {"traces_per_s": round(sat_tps, 1), "p50_ms": round(sat["p50_ms"], 2),
+                       "p99_ms": round(sat["p99_ms"], 2)},
+        "levels": levels, "gen_s": round(gen_s, 1),
     }
     print(json.dumps(line), flush=True)
 

@@ -79,9 +79,16 @@ struct Ctl {
   double sums[8];
 };
 
+// The 6 x 128 reduction lanes have no fixed home: between sift passes they sit
+// at the start of the knot arena; inside a pass, after the spline solve, they
+// reuse PCR buffer 1, which is dead from then on (or follow the PCR buffers
+// when those are smaller than the lanes).
+constexpr int kRedDoubles = 6 * kThreads;
+constexpr size_t kRedBytes = kRedDoubles * sizeof(double);
+
 struct SmemLayout {
   Ctl* ctl;
-  double* red;        // [6][128]
+  double* red;        // [6][128] between passes (= arena start)
   double* imf;        // [N]
   uint32_t* mmax;     // [nch] ballot masks of the last extrema scan
   uint32_t* mmin;
@@ -96,7 +103,6 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(
 __host__ __device__ inline size_t fixed_bytes(int N) {
   size_t nch = (size_t)(N + 31) / 32;
   size_t b = align16(sizeof(Ctl));
-  b += align16(6 * kThreads * sizeof(double));
   b += align16((size_t)N * sizeof(double));
   b += align16(nch * 4) * 2 + align16(nch * 2) * 2;
   return b;
@@ -107,13 +113,13 @@ __device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total) 
   size_t nch = (size_t)(N + 31) / 32;
   char* p = base;
   L.ctl = reinterpret_cast<Ctl*>(p); p += align16(sizeof(Ctl));
-  L.red = reinterpret_cast<double*>(p); p += align16(6 * kThreads * sizeof(double));
   L.imf = reinterpret_cast<double*>(p); p += align16((size_t)N * sizeof(double));
   L.mmax = reinterpret_cast<uint32_t*>(p); p += align16(nch * 4);
   L.mmin = reinterpret_cast<uint32_t*>(p); p += align16(nch * 4);
   L.pmax = reinterpret_cast<uint16_t*>(p); p += align16(nch * 2);
   L.pmin = reinterpret_cast<uint16_t*>(p); p += align16(nch * 2);
   L.arena = p;
+  L.red = reinterpret_cast<double*>(p);
   L.arena_bytes = arena_total - (int)(p - base);
   return L;
 }
@@ -128,11 +134,15 @@ struct Knots {
   double* M[2];
   double* R[2];   // RN(1/h) per knot segment, in buffer 1's a / c arrays
   double* P[2];   // ping-pong PCR buffers: a | b | c | d, each `cap` rows
+  double* red;    // reduction lanes after the solve: buffer 1, or just past it
   int cap;
 };
 
 __host__ __device__ inline size_t knot_bytes(int kc0, int kc1) {
-  return (size_t)(2 * (kc0 + kc1) + 8 * (kc0 + kc1)) * sizeof(double);
+  const int cap = kc0 + kc1;
+  // with EMDB_FAST_DIV buffer 1 holds the segment reciprocals during evaluation
+  const size_t red_extra = (!EMDB_FAST_DIV && 4 * cap >= kRedDoubles) ? 0 : kRedBytes;
+  return (size_t)(2 * cap + 8 * cap) * sizeof(double) + red_extra;
 }
 
 __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
@@ -149,6 +159,7 @@ __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
   K.M[1] = K.P[0] + 2 * K.cap;
   K.R[0] = K.P[1];
   K.R[1] = K.P[1] + 2 * K.cap;
+  K.red = (!EMDB_FAST_DIV && 4 * K.cap >= kRedDoubles) ? K.P[1] : K.P[1] + 4 * K.cap;
   return K;
 }
 
@@ -803,10 +814,23 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       accumulate(ps, old, nw);
     }
   }
-  // per-lane partial sums for the 128-lane trees
-  double* red = L.red;
+  // per-lane partial sums, then the reference's 128-lane trees on warp 0
+  double* red = kSmem ? K.red : L.red;
   red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
   red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
+  __syncthreads();
+  if (warp == 0) {
+    double a0 = lane_tree(red, lane, 0);
+    double a1 = lane_tree(red + 128, lane, 0);
+    double a2 = lane_tree(red + 256, lane, 0);
+    double a3 = lane_tree(red + 384, lane, 0);
+    double a4 = lane_tree(red + 512, lane, 1);
+    double a5 = lane_tree(red + 640, lane, 2);
+    if (lane == 0) {
+      C.sums[0] = a0; C.sums[1] = a1; C.sums[2] = a2;
+      C.sums[3] = a3; C.sums[4] = a4; C.sums[5] = a5;
+    }
+  }
   return (ps.bad ? 1 : 0) | (oor ? 2 : 0);
 }
 
@@ -840,7 +864,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
     T.arange = p.t_mode == kTArange;
     T.T = p.t_mode == kTShared ? p.T : (p.t_mode == kTPerTrace ? p.T + off : nullptr);
 
-    if (fixed_bytes(N) + 64 > (size_t)p.arena_bytes) {
+    if (fixed_bytes(N) + kRedBytes + 64 > (size_t)p.arena_bytes) {
       // cannot hold this trace: report, leave outputs flagged
       if (tid == 0) {
         atomicOr(p.status, kStatusTooLong);
@@ -898,20 +922,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         ++passes;
         const bool pass_bad = (flags & 1) != 0;
         stale |= (flags & 2) != 0;
-        double* red = L.red;
-        __syncthreads();
-        if (warp == 0) {
-          double a0 = lane_tree(red, lane, 0);
-          double a1 = lane_tree(red + 128, lane, 0);
-          double a2 = lane_tree(red + 256, lane, 0);
-          double a3 = lane_tree(red + 384, lane, 0);
-          double a4 = lane_tree(red + 512, lane, 1);
-          double a5 = lane_tree(red + 640, lane, 2);
-          if (lane == 0) {
-            C.sums[0] = a0; C.sums[1] = a1; C.sums[2] = a2;
-            C.sums[3] = a3; C.sums[4] = a4; C.sums[5] = a5;
-          }
-        }
         // ---- post-update extrema scan (also next pass's pre-scan) ----
         e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
         ovf |= e.overflow;
@@ -1093,7 +1103,7 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
     TimeAxis T;
     T.arange = p.t_mode == kTArange;
     T.T = p.t_mode == kTShared ? p.T : (p.t_mode == kTPerTrace ? p.T + off : nullptr);
-    if (fixed_bytes(N) + 64 > (size_t)p.arena_bytes) {
+    if (fixed_bytes(N) + kRedBytes + 64 > (size_t)p.arena_bytes) {
       if (tid == 0) {
         atomicOr(p.status, kStatusTooLong);
         p.degenerate[b] = 1;
@@ -1191,7 +1201,7 @@ cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
   return cudaGetLastError();
 }
 
-size_t sift_fixed_smem(int N) { return fixed_bytes(N); }
+size_t sift_fixed_smem(int N) { return fixed_bytes(N) + kRedBytes; }
 
 size_t sift_slab_bytes(int max_extrema, int nbsym) {
   int kc = max_extrema + 2 * nbsym + 2;
