@@ -35,10 +35,15 @@
 // Tuning knobs (compile-time; results are identical for every setting):
 //  EMDB_EVAL_PAIR  evaluate two samples per loop trip in the fused pass
 //  EMDB_PCR_PAIR   update two PCR rows per loop trip
-//  EMDB_FAST_DIV   reciprocal-based correctly rounded division in evaluation
-// Measured on B200 (cfg1, 16,384 x 2048): all three off is fastest -- the
-// hardware-seeded FP64 division is already short, and the paired loops raise
-// register pressure more than they add overlap.
+//  EMDB_FAST_DIV   reciprocal-based correctly rounded division in evaluation:
+//                  0 none, 1 segment quotients from stored RN(1/h) plus the
+//                  division by 6, 2 the division by 6 only, 3 segment quotients
+//                  from a per-sample RN(1/h) plus the division by 6
+// Measured on B200 (16,384 seismic traces x 2048 samples): the paired loops
+// raise register pressure more than they add overlap; EMDB_FAST_DIV 0/1/2/3
+// ran at 142.5k/154.3k/150.8k/154.9k signals/s, bit-identical outputs.  The
+// gain is the straight-line evaluation: every hardware division carries its
+// own slow-path branch, which splits the sample's independent chains.
 #ifndef EMDB_EVAL_PAIR
 #define EMDB_EVAL_PAIR 0
 #endif
@@ -46,7 +51,7 @@
 #define EMDB_PCR_PAIR 0
 #endif
 #ifndef EMDB_FAST_DIV
-#define EMDB_FAST_DIV 0
+#define EMDB_FAST_DIV 3
 #endif
 
 namespace emdb {
@@ -140,8 +145,8 @@ struct Knots {
 
 __host__ __device__ inline size_t knot_bytes(int kc0, int kc1) {
   const int cap = kc0 + kc1;
-  // with EMDB_FAST_DIV buffer 1 holds the segment reciprocals during evaluation
-  const size_t red_extra = (!EMDB_FAST_DIV && 4 * cap >= kRedDoubles) ? 0 : kRedBytes;
+  // with EMDB_FAST_DIV 1 buffer 1 holds the segment reciprocals during evaluation
+  const size_t red_extra = (EMDB_FAST_DIV != 1 && 4 * cap >= kRedDoubles) ? 0 : kRedBytes;
   return (size_t)(2 * cap + 8 * cap) * sizeof(double) + red_extra;
 }
 
@@ -159,9 +164,41 @@ __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
   K.M[1] = K.P[0] + 2 * K.cap;
   K.R[0] = K.P[1];
   K.R[1] = K.P[1] + 2 * K.cap;
-  K.red = (!EMDB_FAST_DIV && 4 * K.cap >= kRedDoubles) ? K.P[1] : K.P[1] + 4 * K.cap;
+  K.red = (EMDB_FAST_DIV != 1 && 4 * K.cap >= kRedDoubles) ? K.P[1] : K.P[1] + 4 * K.cap;
   return K;
 }
+
+// Split placement, for passes whose knots fit shared memory only without the
+// second PCR buffer: knots X | Y and PCR buffer 0 (which ends up holding the
+// moments) in the arena, buffer 1 in the per-CTA global slab.  Evaluation then
+// reads shared memory only, and half of the PCR levels read the slab.
+__host__ __device__ inline size_t split_bytes(int kc0, int kc1) {
+  return (size_t)(6 * (kc0 + kc1)) * sizeof(double);
+}
+
+__device__ __forceinline__ Knots place_knots_split(char* sbase, int sbytes, char* gbase, int kc0,
+                                                   int kc1) {
+  Knots K;
+  double* p = reinterpret_cast<double*>(sbase);
+  K.X[0] = p; p += kc0;
+  K.Y[0] = p; p += kc0;
+  K.X[1] = p; p += kc1;
+  K.Y[1] = p; p += kc1;
+  K.cap = kc0 + kc1;
+  K.P[0] = p; p += 4 * K.cap;
+  K.P[1] = reinterpret_cast<double*>(gbase);
+  K.M[0] = K.P[0];
+  K.M[1] = K.P[0] + 2 * K.cap;
+  K.R[0] = K.P[1];
+  K.R[1] = K.P[1] + 2 * K.cap;
+  // reduction lanes: shared memory past buffer 0 when they fit, else the slab
+  // (buffer 1 is dead after the solve; the slab holds knot_bytes of the largest pass)
+  if (split_bytes(kc0, kc1) + kRedBytes <= (size_t)sbytes) K.red = p;
+  else K.red = (EMDB_FAST_DIV != 1 && 4 * K.cap >= kRedDoubles) ? K.P[1] : K.P[1] + 4 * K.cap;
+  return K;
+}
+
+enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2 };
 
 // Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 1990):
@@ -171,18 +208,31 @@ __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
 // the second rounds correctly.  Operands whose remainders or quotient could
 // underflow or overflow (|a| or |a*y| outside [2^-900, 2^900], zeros, inf,
 // NaN) take the division.
-// Checked bit for bit against the hardware division by emdb_check_division.
+// A zero numerator gives q0 = a*y, the correctly signed zero (or NaN when y is
+// infinite or NaN, as a/b would be).  Checked bit for bit against the hardware
+// division by emdb_check_division.
+//
+// div_q returns the quotient without branching and sets `slow` for operands
+// outside that range, so a caller can redo a whole sample with the division
+// once instead of branching on every quotient.
 __device__ __noinline__ double div_slow(double a, double b) { return a / b; }
 
-__device__ __forceinline__ double div_rn(double a, double b, double y) {
+__device__ __forceinline__ double div_q(double a, double b, double y, bool& slow) {
   const double q0 = a * y;
   const double e0 = fma(-q0, b, a);
   const double q1 = fma(e0, y, q0);
   const double e1 = fma(-q1, b, a);
   const double q2 = fma(e1, y, q1);
   const double aa = fabs(a), qa = fabs(q0);
-  if (aa > 0x1p-900 && aa < 0x1p+900 && qa > 0x1p-900 && qa < 0x1p+900) return q2;
-  return div_slow(a, b);
+  const bool zero = a == 0.0;
+  slow |= !(zero || (aa > 0x1p-900 && aa < 0x1p+900 && qa > 0x1p-900 && qa < 0x1p+900));
+  return zero ? q0 : q2;
+}
+
+__device__ __forceinline__ double div_rn(double a, double b, double y) {
+  bool slow = false;
+  const double q = div_q(a, b, y, slow);
+  return slow ? div_slow(a, b) : q;
 }
 constexpr double kInv6 = 1.0 / 6.0;   // RN(1/6), folded at compile time
 
@@ -608,7 +658,7 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     const double* x = s0 ? x0b : x1b;
     double Mk1 = Pf[3 * cap + r] / Pf[cap + r];
     M[k + 1] = Mk1;
-#if EMDB_FAST_DIV
+#if EMDB_FAST_DIV == 1
     double* R = s0 ? K.R[0] : K.R[1];
     R[k] = 1.0 / (x[k + 1] - x[k]);
     if (k == mq - 1) R[k + 1] = 1.0 / (x[k + 2] - x[k + 1]);
@@ -655,17 +705,36 @@ __device__ __forceinline__ double eval_seg(const SideView& s, double t, int lo) 
   double y0 = y[lo], y1 = y[lo + 1];
   double M0 = s.M[lo], M1 = s.M[lo + 1];
   double h = x1 - x0;
-#if EMDB_FAST_DIV
-  double rh = s.R[lo];
-  double A = div_rn(x1 - t, h, rh);
-  double B = div_rn(t - x0, h, rh);
-  double num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
-  return (A * y0 + B * y1) + div_rn(num, 6.0, kInv6);
-#else
   double A = (x1 - t) / h;
   double B = (t - x0) / h;
   return A * y0 + B * y1 + ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h) / 6.0;
+}
+
+// eval_seg with the quotients taken from reciprocals (EMDB_FAST_DIV 1..3), in
+// the same operation order; sets `slow` when a quotient needs the division,
+// and the caller then re-evaluates the sample with eval_seg.
+__device__ __forceinline__ double eval_seg_q(const SideView& s, double t, int lo, bool& slow) {
+  if (s.n < 4) return eval_seg(s, t, lo);
+  const double* x = s.x;
+  const double* y = s.y;
+  double x0 = x[lo], x1 = x[lo + 1];
+  double y0 = y[lo], y1 = y[lo + 1];
+  double M0 = s.M[lo], M1 = s.M[lo + 1];
+  double h = x1 - x0;
+#if EMDB_FAST_DIV == 2
+  double A = (x1 - t) / h;
+  double B = (t - x0) / h;
+#else
+#if EMDB_FAST_DIV == 1
+  double rh = s.R[lo];
+#else
+  double rh = 1.0 / h;
 #endif
+  double A = div_q(x1 - t, h, rh, slow);
+  double B = div_q(t - x0, h, rh, slow);
+#endif
+  double num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
+  return (A * y0 + B * y1) + div_q(num, 6.0, kInv6, slow);
 }
 
 // The reference's per-sample binary search (kernels.py:722-726).
@@ -715,16 +784,18 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
 
 // One sift pass after the extrema scan of the current proto-IMF: knots,
 // mirroring, both splines, then the fused envelope / mean / update / partial
-// sums.  kSmem selects shared-memory knot storage (the common case) or the
-// per-CTA global slab, so each instantiation addresses one memory space.
-template <bool kSmem>
+// sums.  kPlace selects where the knots live: shared memory (the common case),
+// split between shared memory and the per-CTA global slab, or the slab alone.
+template <int kPlace>
 __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
                                               int N, int NB, const TimeAxis& T, int tid, int warp,
                                               int lane) {
   Ctl& C = *L.ctl;
   double* imf = L.imf;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
-  Knots K = place_knots(kSmem ? L.arena : slab, kc0, kc1);
+  Knots K = kPlace == kPlaceSmem    ? place_knots(L.arena, kc0, kc1)
+            : kPlace == kPlaceSplit ? place_knots_split(L.arena, L.arena_bytes, slab, kc0, kc1)
+                                    : place_knots(slab, kc0, kc1);
   PassSums ps;
   bool bad = fill_true_knots(L, K, e, N, NB, T, warp, lane);
   bad = __syncthreads_or(bad);
@@ -795,10 +866,24 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     int lo0, lo1, lo0b, lo1b;
     segs(i, t, lo0, lo1);
     if (has2) segs(i2, t2, lo0b, lo1b); else { lo0b = lo0; lo1b = lo1; }
+#if EMDB_FAST_DIV
+    bool slow = false;
+    double emax = eval_seg_q(sv0, t, lo0, slow);
+    double emin = eval_seg_q(sv1, t, lo1, slow);
+    double emax2 = has2 ? eval_seg_q(sv0, t2, lo0b, slow) : 0.0;
+    double emin2 = has2 ? eval_seg_q(sv1, t2, lo1b, slow) : 0.0;
+    if (slow) {
+      emax = eval_seg(sv0, t, lo0);
+      emin = eval_seg(sv1, t, lo1);
+      emax2 = eval_seg(sv0, t2, lo0b);
+      emin2 = eval_seg(sv1, t2, lo1b);
+    }
+#else
     const double emax = eval_seg(sv0, t, lo0);
     const double emin = eval_seg(sv1, t, lo1);
     const double emax2 = eval_seg(sv0, t2, lo0b);
     const double emin2 = eval_seg(sv1, t2, lo1b);
+#endif
     {
       const double mean = 0.5 * (emax + emin);
       const double old = imf[i];
@@ -815,7 +900,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     }
   }
   // per-lane partial sums, then the reference's 128-lane trees on warp 0
-  double* red = kSmem ? K.red : L.red;
+  double* red = kPlace == kPlaceSlab ? L.red : K.red;
   red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
   red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
   __syncthreads();
@@ -914,9 +999,12 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
         int flags;
         if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
-          flags = sift_pass<true>(L, slab, e, N, NB, T, tid, warp, lane);
+          flags = sift_pass<kPlaceSmem>(L, slab, e, N, NB, T, tid, warp, lane);
+        } else if (split_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
+          flags = sift_pass<kPlaceSplit>(L, slab, e, N, NB, T, tid, warp, lane);
+          ++spilled;
         } else {
-          flags = sift_pass<false>(L, slab, e, N, NB, T, tid, warp, lane);
+          flags = sift_pass<kPlaceSlab>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         }
         ++passes;
