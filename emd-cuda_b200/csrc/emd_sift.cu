@@ -43,7 +43,11 @@
 // raise register pressure more than they add overlap; EMDB_FAST_DIV 0/1/2/3
 // ran at 142.5k/154.3k/150.8k/154.9k signals/s, bit-identical outputs.  The
 // gain is the straight-line evaluation: every hardware division carries its
-// own slow-path branch, which splits the sample's independent chains.
+// own slow-path branch, which splits the sample's independent chains.  A
+// branch-free division with no reciprocal at hand (approximate reciprocal,
+// two Newton steps, a Markstein correction and an exact-remainder choice of
+// neighbour) in the PCR rows and the remaining quotients ran slower: 160k vs
+// 180k signals/s -- more instructions than the overlap it buys.
 #ifndef EMDB_EVAL_PAIR
 #define EMDB_EVAL_PAIR 0
 #endif
@@ -118,11 +122,13 @@ __device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total) 
   size_t nch = (size_t)(N + 31) / 32;
   char* p = base;
   L.ctl = reinterpret_cast<Ctl*>(p); p += align16(sizeof(Ctl));
-  L.imf = reinterpret_cast<double*>(p); p += align16((size_t)N * sizeof(double));
   L.mmax = reinterpret_cast<uint32_t*>(p); p += align16(nch * 4);
   L.mmin = reinterpret_cast<uint32_t*>(p); p += align16(nch * 4);
   L.pmax = reinterpret_cast<uint16_t*>(p); p += align16(nch * 2);
   L.pmin = reinterpret_cast<uint16_t*>(p); p += align16(nch * 2);
+  // the proto-IMF directly ahead of the arena: the borrow placement uses both
+  // as one region
+  L.imf = reinterpret_cast<double*>(p); p += align16((size_t)N * sizeof(double));
   L.arena = p;
   L.red = reinterpret_cast<double*>(p);
   L.arena_bytes = arena_total - (int)(p - base);
@@ -198,7 +204,43 @@ __device__ __forceinline__ Knots place_knots_split(char* sbase, int sbytes, char
   return K;
 }
 
-enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2 };
+// Borrow placement, for passes whose knots fit shared memory only together
+// with the proto-IMF's space: the proto-IMF is parked in the per-CTA slab
+// during the solve, PCR buffer 1 takes its place (imf region plus the arena
+// ahead of the knots), and X | Y | buffer 0 sit at the end of the arena, clear
+// of the proto-IMF that the knot fill reads.  Evaluation reads the old sample
+// values back from the slab; the reduction lanes go to the slab after them.
+__host__ __device__ inline bool borrow_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
+                                            int kc1) {
+  const size_t cap = (size_t)(kc0 + kc1);
+  const size_t region = align16((size_t)N * sizeof(double)) + (size_t)arena_bytes;
+  return EMDB_FAST_DIV != 1 && 6 * cap * sizeof(double) <= (size_t)arena_bytes &&
+         10 * cap * sizeof(double) <= region &&
+         (align16((size_t)N * sizeof(double)) + kRedBytes) <= slab_stride;
+}
+
+__device__ __forceinline__ double* borrow_save(char* slab) { return reinterpret_cast<double*>(slab); }
+
+__device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, int arena_bytes,
+                                                    char* slab, int N, int kc0, int kc1) {
+  Knots K;
+  K.cap = kc0 + kc1;
+  double* p = reinterpret_cast<double*>(arena + arena_bytes) - 6 * K.cap;
+  K.X[0] = p; p += kc0;
+  K.Y[0] = p; p += kc0;
+  K.X[1] = p; p += kc1;
+  K.Y[1] = p; p += kc1;
+  K.P[0] = p;
+  K.P[1] = imf;
+  K.M[0] = K.P[0];
+  K.M[1] = K.P[0] + 2 * K.cap;
+  K.R[0] = K.P[1];
+  K.R[1] = K.P[1] + 2 * K.cap;
+  K.red = reinterpret_cast<double*>(slab + align16((size_t)N * sizeof(double)));
+  return K;
+}
+
+enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3 };
 
 // Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 1990):
@@ -794,16 +836,24 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   double* imf = L.imf;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
   Knots K = kPlace == kPlaceSmem    ? place_knots(L.arena, kc0, kc1)
-            : kPlace == kPlaceSplit ? place_knots_split(L.arena, L.arena_bytes, slab, kc0, kc1)
+           : kPlace == kPlaceSplit  ? place_knots_split(L.arena, L.arena_bytes, slab, kc0, kc1)
+           : kPlace == kPlaceBorrow ? place_knots_borrow(imf, L.arena, L.arena_bytes, slab, N, kc0, kc1)
                                     : place_knots(slab, kc0, kc1);
   PassSums ps;
   bool bad = fill_true_knots(L, K, e, N, NB, T, warp, lane);
   bad = __syncthreads_or(bad);
   bool mbad = false;
-  if (warp == 0) mbad = mirror_both(L, K, e, N, NB, T, lane);
+  if (warp == 0) {
+    mbad = mirror_both(L, K, e, N, NB, T, lane);
+  } else if (kPlace == kPlaceBorrow) {
+    // park the proto-IMF while warp 0 mirrors; PCR buffer 1 overwrites it
+    double* save = borrow_save(slab);
+    for (int i = tid - 32; i < N; i += kThreads - 32) save[i] = imf[i];
+  }
   ps.bad = __syncthreads_or(bad || mbad) != 0;
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
   solve_splines(K, kb0, kb1, kn0, kn1, tid);
+  const double* oldv = kPlace == kPlaceBorrow ? borrow_save(slab) : imf;
 
   SideView sv0, sv1;
   sv0.x = K.X[0] + kb0; sv0.y = K.Y[0] + kb0; sv0.M = K.M[0]; sv0.R = K.R[0];
@@ -886,14 +936,14 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
 #endif
     {
       const double mean = 0.5 * (emax + emin);
-      const double old = imf[i];
+      const double old = oldv[i];
       const double nw = old - mean;
       imf[i] = nw;
       accumulate(ps, old, nw);
     }
     if (has2) {
       const double mean = 0.5 * (emax2 + emin2);
-      const double old = imf[i2];
+      const double old = oldv[i2];
       const double nw = old - mean;
       imf[i2] = nw;
       accumulate(ps, old, nw);
@@ -1000,6 +1050,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         int flags;
         if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
           flags = sift_pass<kPlaceSmem>(L, slab, e, N, NB, T, tid, warp, lane);
+        } else if (borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
+          flags = sift_pass<kPlaceBorrow>(L, slab, e, N, NB, T, tid, warp, lane);
+          ++spilled;
         } else if (split_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
           flags = sift_pass<kPlaceSplit>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
