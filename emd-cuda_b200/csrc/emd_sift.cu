@@ -976,6 +976,24 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
 // ---------------------------------------------------------------------------
 // kMinBlocks is the register-budget variant: the compiler fits the kernel
 // into 65536 / (128 * kMinBlocks) registers so that many CTAs can be resident.
+// Chunk completion for the host-memory pipeline (emdb_run_host): after the
+// barrier that follows every output write of trace b, thread 0 counts the
+// trace in its chunk's device counter; the CTA that completes the chunk
+// publishes it with one store to the chunk's flag in mapped host memory, so
+// the host can copy that chunk back while the rest of the batch sifts.  The
+// device fence before the count and the system fence before the flag order
+// all the chunk's output writes (from every CTA that counted) before the flag.
+__device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int tid) {
+  if (p.chunk_count == nullptr || tid != 0) return;
+  __threadfence();
+  const int c = b / p.chunk_traces;
+  const unsigned need = (unsigned)min(p.chunk_traces, p.batch - c * p.chunk_traces);
+  if (atomicAdd(p.chunk_count + c, 1u) + 1u == need) {
+    __threadfence_system();
+    *reinterpret_cast<volatile unsigned*>(p.chunk_flag + c) = 1u;
+  }
+}
+
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftParams p) {
   extern __shared__ __align__(16) char smem[];
@@ -1012,6 +1030,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         p.dbg_nzm[(int64_t)b * MAXI + k] = -1;
       }
       __syncthreads();
+      mark_trace_done(p, b, tid);
       continue;
     }
     SmemLayout L = carve(smem, N, p.arena_bytes);
@@ -1170,6 +1189,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
       p.dbg_nzm[(int64_t)b * MAXI + k] = C.dbg_z[k];
     }
     __syncthreads();
+    mark_trace_done(p, b, tid);
   }
 }
 

@@ -4,10 +4,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/emdb200.h"
 #include "emdb_internal.cuh"
@@ -24,6 +27,15 @@ struct emdb_plan {
   char* d_slab = nullptr;
   size_t slab_stride = 0;
   int slab_ctas = 0;
+  // host-memory pipeline (emdb_run_host): device staging grown on demand, a
+  // non-blocking copy stream, chunk counters and their mapped host flags
+  char* d_stage = nullptr;
+  size_t stage_bytes = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_kernel = nullptr;
+  unsigned* d_chunk_count = nullptr;
+  unsigned* h_chunk_flag = nullptr;   // pinned, mapped
+  unsigned* d_chunk_flag = nullptr;   // its device alias
   std::mutex mu;
 };
 
@@ -193,6 +205,11 @@ int emdb_plan_destroy(emdb_plan* p) {
     if (p->d_slab) cudaFree(p->d_slab);
     if (p->d_ctl) cudaFree(p->d_ctl);
     if (p->d_cnt) cudaFree(p->d_cnt);
+    if (p->d_stage) cudaFree(p->d_stage);
+    if (p->d_chunk_count) cudaFree(p->d_chunk_count);
+    if (p->h_chunk_flag) cudaFreeHost(p->h_chunk_flag);
+    if (p->ev_kernel) cudaEventDestroy(p->ev_kernel);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   }
   delete p;
   return EMDB_OK;
@@ -256,6 +273,138 @@ int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, in
   sp.dbg_ext = dbg_extno;
   sp.dbg_nzm = dbg_nzm;
   return launch_common(p, sp, N, (cudaStream_t)stream);
+}
+
+int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batch, int N,
+                  double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                  int* dbg_nzm, void* stream) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
+  if (batch == 0) return EMDB_OK;
+  if ((N > 0 && (!signals || !imfs)) || !n_imfs || !overflow || !dbg_n || !dbg_extno || !dbg_nzm)
+    return fail(EMDB_ERR_INVALID, "NULL buffer");
+  std::lock_guard<std::mutex> lk(p->mu);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int mi = p->cfg.max_imfs;
+  const size_t B = (size_t)batch, n = (size_t)N;
+  // staging layout: signals | T | imfs | n_imfs | overflow | dbg x3, 256-byte aligned
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t o_sig = 0, o_T = al(o_sig + B * n * 8), o_imf = al(o_T + (T ? n * 8 : 0));
+  const size_t o_n = al(o_imf + B * mi * n * 8), o_ov = al(o_n + B * 4), o_dbg = al(o_ov + B * 4);
+  const size_t dbg_bytes = B * mi * 4, total = o_dbg + 3 * al(dbg_bytes);
+  cudaError_t e;
+  if (total > p->stage_bytes) {
+    if (p->d_stage) cudaFree(p->d_stage);
+    p->d_stage = nullptr;
+    p->stage_bytes = 0;
+    e = cudaMalloc(&p->d_stage, total);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating host-pipeline staging");
+    p->stage_bytes = total;
+  }
+  constexpr int kMaxChunks = 256;
+  if (!p->copy_stream) {
+    e = cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_kernel, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_chunk_count, kMaxChunks * sizeof(unsigned));
+    if (e == cudaSuccess)
+      e = cudaHostAlloc(&p->h_chunk_flag, kMaxChunks * sizeof(unsigned), cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->d_chunk_flag, p->h_chunk_flag, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "setting up the host pipeline");
+  }
+  // chunks of >= 64 traces, at most kMaxChunks of them
+  const int chunk = std::max(64, (batch + kMaxChunks - 1) / kMaxChunks);
+  const int nchunk = (batch + chunk - 1) / chunk;
+  volatile unsigned* flag = p->h_chunk_flag;
+  // the previous call on this plan has returned, so no kernel writes the flags now
+  for (int c = 0; c < nchunk; ++c) flag[c] = 0u;
+
+  char* d = p->d_stage;
+  double* d_sig = reinterpret_cast<double*>(d + o_sig);
+  double* d_T = T ? reinterpret_cast<double*>(d + o_T) : nullptr;
+  double* d_imf = reinterpret_cast<double*>(d + o_imf);
+  int* d_n = reinterpret_cast<int*>(d + o_n);
+  int* d_ov = reinterpret_cast<int*>(d + o_ov);
+  int* d_dn = reinterpret_cast<int*>(d + o_dbg);
+  int* d_de = reinterpret_cast<int*>(d + o_dbg + al(dbg_bytes));
+  int* d_dz = reinterpret_cast<int*>(d + o_dbg + 2 * al(dbg_bytes));
+  e = cudaMemsetAsync(p->d_chunk_count, 0, nchunk * sizeof(unsigned), st);
+  if (e == cudaSuccess && N > 0)
+    e = cudaMemcpyAsync(d_sig, signals, B * n * 8, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && T) e = cudaMemcpyAsync(d_T, T, n * 8, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(e, "host-pipeline input copy");
+
+  emdb::SiftParams sp{};
+  sp.values = d_sig;
+  sp.offsets = nullptr;
+  sp.dense_n = N;
+  sp.T = d_T;
+  sp.t_mode = T ? emdb::kTShared : emdb::kTArange;
+  sp.batch = batch;
+  sp.order = nullptr;
+  sp.imfs = d_imf;
+  sp.n_imfs = d_n;
+  sp.overflow = d_ov;
+  sp.dbg_n = d_dn;
+  sp.dbg_ext = d_de;
+  sp.dbg_nzm = d_dz;
+  sp.chunk_count = p->d_chunk_count;
+  sp.chunk_flag = p->d_chunk_flag;
+  sp.chunk_traces = chunk;
+  int rc = launch_common(p, sp, N, st);
+  if (rc) return rc;
+  e = cudaEventRecord(p->ev_kernel, st);
+  if (e != cudaSuccess) return cuda_fail(e, "host-pipeline event");
+
+  // Copy each chunk's IMF rows back as soon as its flag is up.  Once the
+  // kernel has finished every remaining chunk is copied, so this loop ends
+  // with the kernel whatever the flags say.
+  const size_t row_bytes = (size_t)mi * n * 8;
+  std::string err;
+  std::vector<char> done(nchunk, 0);
+  int left = nchunk;
+  bool kernel_done = false;
+  while (left > 0) {
+    bool moved = false;
+    for (int c = 0; c < nchunk; ++c) {
+      if (done[c] || !(kernel_done || flag[c] != 0u)) continue;
+      const size_t t0 = (size_t)c * chunk, cnt = std::min((size_t)chunk, B - t0);
+      if (row_bytes > 0) {
+        e = cudaMemcpyAsync(reinterpret_cast<char*>(imfs) + t0 * row_bytes,
+                            reinterpret_cast<char*>(d_imf) + t0 * row_bytes, cnt * row_bytes,
+                            cudaMemcpyDeviceToHost, p->copy_stream);
+        if (e != cudaSuccess && err.empty()) err = "IMF copy-back";
+      }
+      done[c] = 1;
+      --left;
+      moved = true;
+    }
+    if (left == 0) break;
+    if (!kernel_done) {
+      e = cudaEventQuery(p->ev_kernel);
+      if (e == cudaSuccess) {
+        kernel_done = true;
+        continue;
+      }
+      if (e != cudaErrorNotReady) {
+        cudaStreamSynchronize(p->copy_stream);
+        return cuda_fail(e, "sift kernel");
+      }
+    }
+    if (!moved) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  // per-trace counts and debug rows after the whole kernel
+  e = cudaStreamWaitEvent(p->copy_stream, p->ev_kernel, 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(n_imfs, d_n, B * 4, cudaMemcpyDeviceToHost, p->copy_stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(overflow, d_ov, B * 4, cudaMemcpyDeviceToHost, p->copy_stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dbg_n, d_dn, dbg_bytes, cudaMemcpyDeviceToHost, p->copy_stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dbg_extno, d_de, dbg_bytes, cudaMemcpyDeviceToHost, p->copy_stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dbg_nzm, d_dz, dbg_bytes, cudaMemcpyDeviceToHost, p->copy_stream);
+  cudaError_t e2 = cudaStreamSynchronize(p->copy_stream);
+  if (e != cudaSuccess) return cuda_fail(e, "host-pipeline result copy");
+  if (e2 != cudaSuccess) return cuda_fail(e2, "host-pipeline copy stream");
+  if (!err.empty()) return fail(EMDB_ERR_CUDA, err);
+  return EMDB_OK;
 }
 
 int emdb_run_ragged(emdb_plan* p, const double* values, const int64_t* offsets, int batch,

@@ -43,6 +43,11 @@ struct SiftParams {
   char* slab;                 // per-CTA global spill area
   size_t slab_stride;         // bytes per CTA
   int arena_bytes;            // dynamic shared memory per CTA
+  // chunk completion for copying finished traces back early (NULL = off):
+  // traces [c*chunk_traces, (c+1)*chunk_traces) form chunk c
+  unsigned* chunk_count;      // device counters, zeroed before launch
+  unsigned* chunk_flag;       // mapped host flags, set to 1 when chunk c is complete
+  int chunk_traces;
   // config (EMDKernelConfig fields)
   int max_extrema;
   int nbsym;

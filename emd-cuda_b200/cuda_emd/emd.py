@@ -81,7 +81,12 @@ class GPUBatchEMD:
                 stacklevel=3,
             )
 
-    def __call__(self, signals, T=None):
+    def __call__(self, signals, T=None, out=None):
+        """Decompose signals [batch, N] (or [N]).  Device input (torch CUDA,
+        CuPy) gives device results.  Host input (NumPy, CPU torch) runs the
+        host pipeline: one launch whose finished traces are copied back while
+        the rest sift, results in host memory; ``out`` = optional
+        (imfs, n_imfs, overflow) host buffers to fill."""
         if signals.ndim == 1:
             signals = signals[None, :]
         dt = np.dtype(str(signals.dtype).replace("torch.", ""))
@@ -94,7 +99,13 @@ class GPUBatchEMD:
         launcher = self._get_launcher()
         batch, N = signals.shape
         Tn = _normalise_T(T, N, launcher.device)
-        imfs, n_imfs, overflow, dn, de, dz = launcher.run(signals, Tn)
+        from ._arrays import kind_of
+        if kind_of(signals) in ("numpy", "torch_cpu"):
+            imfs, n_imfs, overflow, dn, de, dz = launcher.run_host(signals, Tn, out=out)
+        elif out is not None:
+            raise ValueError("out= is for host input; device input returns device arrays")
+        else:
+            imfs, n_imfs, overflow, dn, de, dz = launcher.run(signals, Tn)
         self.last_debug = (dn, de, dz)
         launcher.check_status()
         self._overflow_warning(overflow, batch)

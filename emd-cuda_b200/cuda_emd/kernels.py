@@ -14,7 +14,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from ._arrays import as_device_f64, as_device_i64, as_device_i32, to_caller, device_of, stream_of
+from ._arrays import (as_device_f64, as_device_i64, as_device_i32, to_caller, device_of, stream_of,
+                      kind_of)
 
 
 @dataclass
@@ -147,6 +148,52 @@ class EMDBatchLauncher:
             dz.data_ptr(), st), "emdb_run")
         self._keepalive = (sig, Td)
         return tuple(to_caller(x, kind) for x in (imfs, n_imfs, ovf, dn, de, dz))
+
+    def run_host(self, signals, T, out=None):
+        """Dense batch from and to host memory (NumPy or CPU torch) through
+        emdb_run_host: one launch, each finished chunk's IMF rows copied back
+        while the rest still sifts.  ``out`` = optional (imfs, n_imfs, overflow)
+        host buffers to fill (page-locked ones keep the copies asynchronous);
+        otherwise page-locked buffers are allocated.  Returns the same 6-tuple
+        as run(), in the caller's framework."""
+        import torch
+        self._check_dtype(signals, T)
+        kind = kind_of(signals)
+        if kind not in ("numpy", "torch_cpu"):
+            raise ValueError("run_host takes host arrays (NumPy or CPU torch)")
+        sig = signals if isinstance(signals, torch.Tensor) else torch.from_numpy(np.asarray(signals))
+        sig = sig.contiguous()
+        if sig.dim() != 2:
+            raise ValueError("signals must be [batch, N]")
+        B, N = sig.shape
+        mi = self.config.max_imfs
+        Th = None
+        if T is not None:
+            Th = (T.detach().cpu() if isinstance(T, torch.Tensor)
+                  else torch.from_numpy(np.asarray(T, dtype=np.float64))).contiguous()
+
+        def host(shape, dtype, given, what):
+            if given is None:
+                return torch.empty(shape, dtype=dtype, pin_memory=True)
+            t = given if isinstance(given, torch.Tensor) else torch.from_numpy(given)
+            if t.is_cuda or tuple(t.shape) != shape or t.dtype != dtype or not t.is_contiguous():
+                raise ValueError(f"out {what} must be a contiguous host {dtype} array of shape {shape}")
+            return t
+
+        o = out if out is not None else (None, None, None)
+        imfs = host((B, mi, N), torch.float64, o[0], "imfs")
+        n_imfs = host((B,), torch.int32, o[1], "n_imfs")
+        ovf = host((B,), torch.int32, o[2], "overflow")
+        dn, de, dz = (torch.empty((B, mi), dtype=torch.int32, pin_memory=True) for _ in range(3))
+        st = stream_of(torch.device("cuda", self.device))
+        _native.check(self._plan.L.emdb_run_host(
+            self._plan.handle, sig.data_ptr(), Th.data_ptr() if Th is not None else None, B, N,
+            imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(), dn.data_ptr(), de.data_ptr(),
+            dz.data_ptr(), st), "emdb_run_host")
+        res = (imfs, n_imfs, ovf, dn, de, dz)
+        if kind == "numpy":
+            return tuple(x.numpy() for x in res)
+        return res
 
     def run_ragged(self, values, offsets, order=None, T=None, t_per_trace: bool = True,
                    max_n: int | None = None):

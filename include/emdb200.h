@@ -83,6 +83,19 @@ int emdb_run(emdb_plan* plan, const double* signals, const double* T, int batch,
              double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
              int* dbg_nzm, void* stream);
 
+/* emdb_run with every pointer in HOST memory (the reference's GPUBatchEMD
+ * called on NumPy input, emd.py:71-107, which copies in, runs and leaves the
+ * copy-back to the caller).  Inputs go up on `stream`, one sift launch covers
+ * the batch, and the IMF rows of each finished chunk of traces come back on
+ * the plan's own copy stream while the rest still sifts; counts and debug
+ * rows follow the kernel.  Returns once every output is in host memory.
+ * Page-locked host buffers make the copies asynchronous; pageable ones work
+ * but serialise them.  Device staging (inputs + outputs) is plan-owned and
+ * grows to the largest batch seen. */
+int emdb_run_host(emdb_plan* plan, const double* signals, const double* T, int batch, int N,
+                  double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                  int* dbg_nzm, void* stream);
+
 /* CSR batch of mixed lengths in one launch: trace b is
  * values[offsets[b] .. offsets[b+1]), offsets is a DEVICE int64 [batch+1]
  * array, max_n = max trace length (host value, sizes the arena).
