@@ -824,11 +824,50 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
   ps.omin = fmin(ps.omin, old);
 }
 
+// RN(1/h) for integer h in [1, kRcpTab], built at compile time by IEEE
+// division and shipped initialised in the module.
+constexpr int kRcpTab = 16384;
+struct RcpTab { double v[kRcpTab + 1]; };
+constexpr RcpTab make_rcp_tab() {
+  RcpTab t{};
+  for (int h = 1; h <= kRcpTab; ++h) t.v[h] = 1.0 / (double)h;
+  return t;
+}
+__device__ const RcpTab g_rcp = make_rcp_tab();
+
+// eval_seg for the time axis T = arange(N): knot positions (true and
+// mirrored) and sample times are integers, so A = (x1-t)/h and B = (t-x0)/h
+// are quotients of integers 0 <= a <= h.  For those, q0 = RN(a*y) with
+// y = RN(1/h) and one correction RN(q0 + (a - h*q0)*y) equal RN(a/h): checked
+// exhaustively for every pair with h <= 65536 (2.1e9 pairs).  Anything outside
+// (h beyond the table, a not in [0, h]) sets `slow`, and the caller redoes the
+// sample with eval_seg.  Same operation order as eval_seg otherwise.
+__device__ __forceinline__ double eval_seg_int(const SideView& s, double t, int lo, bool& slow) {
+  if (s.n < 4) return eval_seg(s, t, lo);
+  const double* x = s.x;
+  const double* y = s.y;
+  double x0 = x[lo], x1 = x[lo + 1];
+  double y0 = y[lo], y1 = y[lo + 1];
+  double M0 = s.M[lo], M1 = s.M[lo + 1];
+  double h = x1 - x0;
+  const double a = x1 - t, b = t - x0;
+  const bool in = h >= 1.0 && h <= (double)kRcpTab && a >= 0.0 && b >= 0.0 && a <= h && b <= h;
+  const int hi = in ? (int)h : 1;
+  slow |= !in || (double)hi != h;
+  const double r = g_rcp.v[hi];
+  double A = a * r;
+  A = fma(fma(-A, h, a), r, A);
+  double B = b * r;
+  B = fma(fma(-B, h, b), r, B);
+  double num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
+  return (A * y0 + B * y1) + div_q(num, 6.0, kInv6, slow);
+}
+
 // One sift pass after the extrema scan of the current proto-IMF: knots,
 // mirroring, both splines, then the fused envelope / mean / update / partial
 // sums.  kPlace selects where the knots live: shared memory (the common case),
 // split between shared memory and the per-CTA global slab, or the slab alone.
-template <int kPlace>
+template <int kPlace, bool kInt>
 __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
                                               int N, int NB, const TimeAxis& T, int tid, int warp,
                                               int lane) {
@@ -918,10 +957,22 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     if (has2) segs(i2, t2, lo0b, lo1b); else { lo0b = lo0; lo1b = lo1; }
 #if EMDB_FAST_DIV
     bool slow = false;
-    double emax = eval_seg_q(sv0, t, lo0, slow);
-    double emin = eval_seg_q(sv1, t, lo1, slow);
-    double emax2 = has2 ? eval_seg_q(sv0, t2, lo0b, slow) : 0.0;
-    double emin2 = has2 ? eval_seg_q(sv1, t2, lo1b, slow) : 0.0;
+    double emax, emin, emax2 = 0.0, emin2 = 0.0;
+    if (kInt) {
+      emax = eval_seg_int(sv0, t, lo0, slow);
+      emin = eval_seg_int(sv1, t, lo1, slow);
+      if (has2) {
+        emax2 = eval_seg_int(sv0, t2, lo0b, slow);
+        emin2 = eval_seg_int(sv1, t2, lo1b, slow);
+      }
+    } else {
+      emax = eval_seg_q(sv0, t, lo0, slow);
+      emin = eval_seg_q(sv1, t, lo1, slow);
+      if (has2) {
+        emax2 = eval_seg_q(sv0, t2, lo0b, slow);
+        emin2 = eval_seg_q(sv1, t2, lo1b, slow);
+      }
+    }
     if (slow) {
       emax = eval_seg(sv0, t, lo0);
       emin = eval_seg(sv1, t, lo1);
@@ -994,7 +1045,7 @@ __device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int 
   }
 }
 
-template <int kMinBlocks>
+template <int kMinBlocks, bool kInt>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftParams p) {
   extern __shared__ __align__(16) char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1068,15 +1119,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
         int flags;
         if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
-          flags = sift_pass<kPlaceSmem>(L, slab, e, N, NB, T, tid, warp, lane);
+          flags = sift_pass<kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
         } else if (borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
-          flags = sift_pass<kPlaceBorrow>(L, slab, e, N, NB, T, tid, warp, lane);
+          flags = sift_pass<kPlaceBorrow, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         } else if (split_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
-          flags = sift_pass<kPlaceSplit>(L, slab, e, N, NB, T, tid, warp, lane);
+          flags = sift_pass<kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         } else {
-          flags = sift_pass<kPlaceSlab>(L, slab, e, N, NB, T, tid, warp, lane);
+          flags = sift_pass<kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         }
         ++passes;
@@ -1370,21 +1421,37 @@ size_t sift_slab_bytes(int max_extrema, int nbsym) {
 }
 
 namespace {
+// kInt: the kernel build for the integer time axis (T = arange), whose
+// segment quotients use the reciprocal table.
+template <int V, bool kInt>
+cudaError_t occupancy_vt(int arena_bytes, int* ctas_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V, kInt>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, arena_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_sift_kernel<V, kInt>,
+                                                       kThreads, arena_bytes);
+}
+// CTAs per SM that both builds reach (the smaller), so a plan's grid fits either
 template <int V>
 cudaError_t occupancy_v(int arena_bytes, int* ctas_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       arena_bytes);
+  int a = 0, b = 0;
+  cudaError_t e = occupancy_vt<V, true>(arena_bytes, &a);
+  if (e == cudaSuccess) e = occupancy_vt<V, false>(arena_bytes, &b);
+  *ctas_per_sm = a < b ? a : b;
+  return e;
+}
+template <int V, bool kInt>
+cudaError_t launch_vt(const SiftParams& p, int grid, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V, kInt>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, p.arena_bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_sift_kernel<V>, kThreads,
-                                                       arena_bytes);
+  emd_sift_kernel<V, kInt><<<grid, kThreads, p.arena_bytes, stream>>>(p);
+  return cudaGetLastError();
 }
 template <int V>
 cudaError_t launch_v(const SiftParams& p, int grid, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       p.arena_bytes);
-  if (e != cudaSuccess) return e;
-  emd_sift_kernel<V><<<grid, kThreads, p.arena_bytes, stream>>>(p);
-  return cudaGetLastError();
+  return p.t_mode == kTArange ? launch_vt<V, true>(p, grid, stream)
+                              : launch_vt<V, false>(p, grid, stream);
 }
 }  // namespace
 

@@ -248,6 +248,12 @@ int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm,
   return EMDB_OK;
 }
 
+int emdb_min_arena(int max_n, int* arena_bytes) {
+  if (max_n < 0 || !arena_bytes) return fail(EMDB_ERR_INVALID, "bad arguments");
+  *arena_bytes = (int)((emdb::sift_fixed_smem(std::max(max_n, 1)) + 64 + 15) & ~size_t(15));
+  return EMDB_OK;
+}
+
 int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, int N,
              double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
              void* stream) {

@@ -28,7 +28,7 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
-           "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host")
+           "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -63,6 +63,7 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
+        L.emdb_min_arena.argtypes = [I, ctypes.POINTER(I)]
         L.emdb_run_ragged.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]
         L.emdb_envelope.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
         L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
@@ -134,6 +135,12 @@ class Plan:
         check(self.L.emdb_plan_query(self.handle, int(max_n), ctypes.byref(a), ctypes.byref(c),
                                      ctypes.byref(g)), "emdb_plan_query")
         return a.value, c.value, g.value
+
+    def min_arena(self, max_n: int) -> int:
+        """Smallest arena that holds a trace of max_n samples (knots all spilled)."""
+        a = ctypes.c_int()
+        check(self.L.emdb_min_arena(int(max_n), ctypes.byref(a)), "emdb_min_arena")
+        return a.value
 
     def counters(self, reset: bool = False) -> tuple[int, int]:
         """(sift passes, passes spilled to the global slab) since creation / last reset."""

@@ -15,8 +15,9 @@ longest-predicted-first.  Order never changes a result.
 
 The autotuner times every candidate (register-budget variant, arena) pair --
 the largest arena that keeps k = 6..1 CTAs per SM resident, with the kernel
-build compiled for max(k, 4) CTAs -- on a sample of each tier and caches the
-winner in a JSON file keyed by device, config and tier.
+build compiled for max(k, 4) CTAs -- on a sample of each tier large enough to
+measure throughput (about 16 traces per CTA, or the whole tier) and caches
+the winner in a JSON file keyed by device, config and tier.
 """
 from __future__ import annotations
 
@@ -44,17 +45,17 @@ def tier_of(n: int) -> int:
 def candidates(plan: _native.Plan, max_n: int) -> list[tuple[int, int]]:
     """(register variant, arena) pairs worth trying for traces up to max_n:
     the largest arena that keeps k CTAs per SM resident, k = 6..1, with the
-    register-budget build for max(k, 4) CTAs, if the arena holds the trace."""
+    register-budget build for max(k, 4) CTAs, if the arena holds the trace
+    (even with every knot spilled: more resident CTAs can beat on-chip knots,
+    e.g. 3 CTAs/SM for 8192-sample seismic traces)."""
     plan.set_variant(4)
     plan.set_arena(0)
-    auto, _, _ = plan.query(max_n)            # smallest arena that holds a trace
+    floor = plan.min_arena(max_n)
     out = []
     for k in (6, 5, 4, 3, 2, 1):
         a = min((SMEM_PER_SM // k - CTA_RESERVED) & ~15, 232448)
-        if auto > 0 and a >= auto:
+        if a >= floor:
             out.append((max(k, 4), a))
-    if not out and auto > 0:
-        out.append((4, auto))
     return out
 
 
@@ -94,7 +95,8 @@ class RaggedRunner:
         import torch
         name = torch.cuda.get_device_name(self.device)
         c = self.cfg
-        return f"{name}|{c.max_extrema},{c.nbsym},{c.max_iteration},{c.max_imfs}|{edge}"
+        # "t2": entries timed on throughput-sized samples (older ones are ignored)
+        return f"t2|{name}|{c.max_extrema},{c.nbsym},{c.max_iteration},{c.max_imfs}|{edge}"
 
     def _load_cache(self) -> dict:
         if self.cache_path and os.path.isfile(self.cache_path):
@@ -133,8 +135,12 @@ class RaggedRunner:
         chosen = {}
         for t in tiers:
             key = self._key(t.edge)
-            if key in self._cache:
-                c = self._cache[key]
+            sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+            want = sample or min(t.idx.size, 16 * 6 * sms)
+            c = self._cache.get(key)
+            # a tuning measured on a much smaller batch than this tier's sample
+            # is redone (small samples time their longest trace, not throughput)
+            if c is not None and 2 * int(c.get("sample", 0)) >= want:
                 t.set_tuning(c.get("variant", 4), c["arena"])
                 chosen[t.edge] = c
                 continue
@@ -145,13 +151,19 @@ class RaggedRunner:
                 v4 = [c for c in cands if c[0] == 4]
                 t.set_tuning(*(v4[0] if v4 else cands[0]))
                 continue
-            n_s = sample or min(t.idx.size, 6 * 148 * 3)
+            # Throughput, not a small sample's makespan: with per-trace costs
+            # spread over two orders of magnitude, a sample of a few traces per
+            # CTA finishes with its single longest trace, which favours fewer,
+            # faster CTAs.  So the sample fills the densest candidate's CTAs
+            # ~16 times over (or is the whole tier).
+            n_s = want
             sub = torch.from_numpy(t.idx[:n_s].astype(np.int32)).to(values.device)
+            warm = sub[:64]
             res = {}
             outs = self._alloc_out(values, offsets)
             for v, a in cands:
                 t.set_tuning(v, a)
-                self._launch_tier(t, values, offsets, sub, outs)       # warm
+                self._launch_tier(t, values, offsets, warm, outs)      # first-launch set-up
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record()

@@ -73,6 +73,12 @@ int emdb_plan_set_variant(emdb_plan* plan, int min_ctas_per_sm);
 /* Arena and CTAs/SM the plan would use for traces up to max_n. */
 int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
                     int* grid_max);
+/* Smallest arena (bytes) that holds a trace of max_n samples: its proto-IMF,
+ * control block and scan masks; every knot then lives in the global slab.
+ * No reference counterpart (the reference sizes one fixed knot buffer per
+ * block, EMDKernelConfig.shared_mem_bytes, kernels.py:1273-1275); the
+ * autotuner uses it as the floor of its candidates. */
+int emdb_min_arena(int max_n, int* arena_bytes);
 
 /* Dense batch, the reference's run(): signals [batch, N], T [N] or NULL
  * (= arange(N), already normalised as emd.py:83-88 does), outputs

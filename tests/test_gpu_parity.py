@@ -29,21 +29,36 @@ def _cfg(c):
                            max_imfs=int(c[3]), threads_per_block=int(c[4]))
 
 
-def _run_np(cfg, X, T):
+def _run_np(cfg, X, T, axis="given"):
+    """Run the dense launcher.  axis="given" passes T as an array (the general
+    time-axis kernel); axis="arange" passes None, which selects the kernel
+    build for the integer axis T = arange(N) -- only valid when T is that."""
     import torch
     L = cfg.build()
     sig = torch.from_numpy(np.ascontiguousarray(X)).cuda()
-    Td = torch.from_numpy(np.ascontiguousarray(T)).cuda()
+    if axis == "arange":
+        assert np.array_equal(T, np.arange(X.shape[1], dtype=np.float64))
+        Td = None
+    else:
+        Td = torch.from_numpy(np.ascontiguousarray(T)).cuda()
     out = L.run(sig, Td)
     L.check_status()
     return [o.cpu().numpy() for o in out]
 
 
+def _axes(T, N):
+    """Both kernel builds when T is arange(N), else the general one."""
+    return ("given", "arange") if np.array_equal(T, np.arange(N, dtype=np.float64)) else ("given",)
+
+
 @pytest.mark.parametrize("name", [g["name"] for g in cases.groups()])
-def test_golden_bitexact(golden, name):
+@pytest.mark.parametrize("axis", ["given", "arange"])
+def test_golden_bitexact(golden, name, axis):
     X = golden[f"{name}__signals"]
     T = golden[f"{name}__T"]
-    imfs, n_imfs, ovf, dn, de, dz = _run_np(_cfg(golden[f"{name}__cfg"]), X, T)
+    if axis not in _axes(T, X.shape[1]):
+        pytest.skip("time axis is not arange")
+    imfs, n_imfs, ovf, dn, de, dz = _run_np(_cfg(golden[f"{name}__cfg"]), X, T, axis)
     for b in range(X.shape[0]):
         assert n_imfs[b] == golden[f"{name}__nofma__n_imfs"][b], (name, b)
         assert ovf[b] == golden[f"{name}__nofma__overflow"][b], (name, b)
@@ -100,14 +115,34 @@ def test_oracle_fresh_inputs():
     from oracle import emd_oracle as O
     for X in (W.sinusoid_batch(12, 1024, seed=100), W.seismic_batch(4, 2048, seed=101)):
         T = np.arange(X.shape[1], dtype=np.float64)
-        imfs, n_imfs, ovf, dn, de, dz = _run_np(EMDKernelConfig(), X, T)
-        for b in range(X.shape[0]):
-            r = O.emd_signal(X[b], T)
+        refs = [O.emd_signal(X[b], T) for b in range(X.shape[0])]
+        for axis in ("given", "arange"):
+            imfs, n_imfs, ovf, dn, de, dz = _run_np(EMDKernelConfig(), X, T, axis)
+            for b, r in enumerate(refs):
+                assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
+                np.testing.assert_array_equal(dn[b], r.debug_n)
+                np.testing.assert_array_equal(de[b], r.debug_extno)
+                np.testing.assert_array_equal(dz[b], r.debug_nzm)
+                assert _sha(imfs[b]) == _sha(r.imfs), (axis, b)
+
+
+def test_long_knot_spacing_matches_oracle():
+    """Smooth long traces: knot spacings beyond the integer axis's reciprocal
+    table (16384 samples; these reach ~23,800) take the exact fallback inside
+    that build; both builds equal the oracle bit for bit."""
+    from cuda_emd import EMDKernelConfig
+    from oracle import emd_oracle as O
+    N = 24000
+    t = np.arange(N, dtype=np.float64)
+    X = np.stack([np.sin(2 * np.pi * t / 30000.0) + 0.2 * np.sin(2 * np.pi * t / 2500.0 + 0.3) + 1e-5 * t,
+                  np.cos(2 * np.pi * t / 24000.0) + 0.1 * np.sin(2 * np.pi * t / 700.0)])
+    refs = [O.emd_signal(X[b], t) for b in range(2)]
+    for axis in ("given", "arange"):
+        imfs, n_imfs, ovf, dn, de, dz = _run_np(EMDKernelConfig(), X, t, axis)
+        for b, r in enumerate(refs):
             assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
             np.testing.assert_array_equal(dn[b], r.debug_n)
-            np.testing.assert_array_equal(de[b], r.debug_extno)
-            np.testing.assert_array_equal(dz[b], r.debug_nzm)
-            assert _sha(imfs[b]) == _sha(r.imfs)
+            assert _sha(imfs[b]) == _sha(r.imfs), (axis, b)
 
 
 def test_ragged_matches_oracle_and_order():
@@ -190,13 +225,14 @@ def test_nbsym_variants_match_oracle(nbsym):
     X = W.sinusoid_batch(8, 512, seed=200 + nbsym)
     T = np.arange(512, dtype=np.float64)
     cfg = EMDKernelConfig(nbsym=nbsym)
-    imfs, n_imfs, ovf, dn, de, dz = _run_np(cfg, X, T)
     ocfg = O.OracleConfig(nbsym=nbsym)
-    for b in range(X.shape[0]):
-        r = O.emd_signal(X[b], T, ocfg)
-        assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
-        np.testing.assert_array_equal(dn[b], r.debug_n)
-        assert _sha(imfs[b]) == _sha(r.imfs), (nbsym, b)
+    refs = [O.emd_signal(X[b], T, ocfg) for b in range(X.shape[0])]
+    for axis in ("given", "arange"):
+        imfs, n_imfs, ovf, dn, de, dz = _run_np(cfg, X, T, axis)
+        for b, r in enumerate(refs):
+            assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow
+            np.testing.assert_array_equal(dn[b], r.debug_n)
+            assert _sha(imfs[b]) == _sha(r.imfs), (nbsym, axis, b)
 
 
 @pytest.mark.parametrize("arena", [0, 26000, 232448])
