@@ -35,6 +35,14 @@
 // Tuning knobs (compile-time; results are identical for every setting):
 //  EMDB_EVAL_PAIR  evaluate two samples per loop trip in the fused pass
 //  EMDB_PCR_PAIR   update two PCR rows per loop trip
+//  EMDB_MERGED_PLACE  0: one sift-pass instance per knot placement; 1: one
+//                  for the on-chip placements and one for the off-chip ones
+//                  (placement chosen at run time); 2: one for all
+//  EMDB_TREE_SPLIT the six end-of-pass reduction trees spread over the warps
+// Same B200, same clocks, 16,384 x 2048 seismic: MERGED_PLACE/TREE_SPLIT
+// 1/1 208.4k signals/s, 1/0 188.1k, 2/1 195.6k, 0/0 184.9k (and 0/1 172.7k on
+// another box against 208.2k for 1/1): less sift-pass code relieves
+// instruction supply, the dominant stall after FP64 latency.
 //  EMDB_FAST_DIV   reciprocal-based correctly rounded division in evaluation:
 //                  0 none, 1 segment quotients from stored RN(1/h) plus the
 //                  division by 6, 2 the division by 6 only, 3 segment quotients
@@ -56,6 +64,12 @@
 #endif
 #ifndef EMDB_FAST_DIV
 #define EMDB_FAST_DIV 3
+#endif
+#ifndef EMDB_MERGED_PLACE
+#define EMDB_MERGED_PLACE 1
+#endif
+#ifndef EMDB_TREE_SPLIT
+#define EMDB_TREE_SPLIT 1
 #endif
 
 namespace emdb {
@@ -241,6 +255,7 @@ __device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, in
 }
 
 enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3 };
+enum : int { kOnChip = -1, kOffChip = -2, kAnyPlace = -3 };
 
 // Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 1990):
@@ -867,10 +882,17 @@ __device__ __forceinline__ double eval_seg_int(const SideView& s, double t, int 
 // mirroring, both splines, then the fused envelope / mean / update / partial
 // sums.  kPlace selects where the knots live: shared memory (the common case),
 // split between shared memory and the per-CTA global slab, or the slab alone.
-template <int kPlace, bool kInt>
+template <int kGroup, bool kInt>
 __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
                                               int N, int NB, const TimeAxis& T, int tid, int warp,
-                                              int lane) {
+                                              int lane, int place = kPlaceSmem) {
+  // kGroup >= 0: one placement, fixed at compile time.  kGroup == kOnChip /
+  // kOffChip: one instance for the on-chip (shared, borrow) or off-chip
+  // (split, slab) placements, chosen by `place` at run time.
+  const int kPlace = kGroup >= 0 ? kGroup
+                   : kGroup == kOnChip ? (place == kPlaceBorrow ? kPlaceBorrow : kPlaceSmem)
+                   : kGroup == kOffChip ? (place == kPlaceSplit ? kPlaceSplit : kPlaceSlab)
+                                        : place;
   Ctl& C = *L.ctl;
   double* imf = L.imf;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
@@ -1005,6 +1027,18 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
   red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
   __syncthreads();
+#if EMDB_TREE_SPLIT
+  // the six trees spread over the warps (warp w: sum w; warps 0/1 also the
+  // max / min tree); the next extrema scan's barrier publishes C.sums
+  {
+    const double a = lane_tree(red + 128 * warp, lane, 0);
+    if (lane == 0) C.sums[warp] = a;
+    if (warp < 2) {
+      const double b = lane_tree(red + 128 * (4 + warp), lane, 1 + warp);
+      if (lane == 0) C.sums[4 + warp] = b;
+    }
+  }
+#else
   if (warp == 0) {
     double a0 = lane_tree(red, lane, 0);
     double a1 = lane_tree(red + 128, lane, 0);
@@ -1017,6 +1051,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       C.sums[3] = a3; C.sums[4] = a4; C.sums[5] = a5;
     }
   }
+#endif
   return (ps.bad ? 1 : 0) | (oor ? 2 : 0);
 }
 
@@ -1118,6 +1153,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         }
         const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
         int flags;
+#if EMDB_MERGED_PLACE
+        {
+          const int place = knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSmem
+                          : borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlaceBorrow
+                          : split_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSplit
+                                                                         : kPlaceSlab;
+          if (EMDB_MERGED_PLACE == 2)
+            flags = sift_pass<kAnyPlace, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
+          else if (place == kPlaceSmem || place == kPlaceBorrow)
+            flags = sift_pass<kOnChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
+          else
+            flags = sift_pass<kOffChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
+          spilled += place != kPlaceSmem;
+        }
+#else
         if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
           flags = sift_pass<kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
         } else if (borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
@@ -1130,6 +1180,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
           flags = sift_pass<kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         }
+#endif
         ++passes;
         const bool pass_bad = (flags & 1) != 0;
         stale |= (flags & 2) != 0;
