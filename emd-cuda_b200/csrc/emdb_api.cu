@@ -76,7 +76,9 @@ int auto_arena(const emdb_plan* p, int max_n) {
   for (int want = p->variant; want >= 1; --want) {
     int arena = per_sm / want - 1024;
     arena = std::min(arena, p->smem_optin);
-    arena &= ~15;
+    // shared memory is allocated in 128-byte units: a 16-byte-rounded share
+    // can round up past the SM's capacity and lose a CTA (e.g. 5 per SM)
+    arena &= ~127;
     // need the fixed part plus room for ~2 x 96 knots before spilling
     size_t min_need = fixed + (size_t)(11 * 2 * (96 + 2 * p->cfg.nbsym + 2)) * sizeof(double);
     if ((size_t)arena >= min_need) { best = arena; break; }

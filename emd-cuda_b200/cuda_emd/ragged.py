@@ -53,7 +53,9 @@ def candidates(plan: _native.Plan, max_n: int) -> list[tuple[int, int]]:
     floor = plan.min_arena(max_n)
     out = []
     for k in (6, 5, 4, 3, 2, 1):
-        a = min((SMEM_PER_SM // k - CTA_RESERVED) & ~15, 232448)
+        # 128-byte units: shared memory is allocated in those, so a 16-byte
+        # rounded share can round up past the SM and lose a CTA
+        a = min((SMEM_PER_SM // k - CTA_RESERVED) & ~127, 232448)
         if a >= floor:
             out.append((max(k, 4), a))
     return out
