@@ -190,6 +190,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--requests", type=int, default=160, help="serve: requests per load level")
     ap.add_argument("--loads", default="0.1,0.3,0.5,0.7,0.9,1.1", help="serve: offered loads")
+    ap.add_argument("--ref-sample", type=int, default=4096,
+                    help="reference arm, ragged64k: traces per padded GPU measurement")
     a = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -381,55 +383,103 @@ def main():
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libemd_ref.so")
 
 
+def cpu_reference_steps(X: np.ndarray, pool, cores: int, steps: int, warmup: int, per: int):
+    """The reference arm's CPU timing: `warmup` untimed and `steps` timed steps,
+    each the oracle on a bounded slice of `per` traces (successive slices,
+    wrapping), all host cores.  Returns (signals/s, traces timed, wall s)."""
+    B = X.shape[0]
+    per = max(1, min(per, B))
+
+    def step(k):
+        s0 = (k * per) % B
+        sl = X[s0:s0 + per] if s0 + per <= B else np.concatenate([X[s0:], X[:s0 + per - B]])
+        return cpu_oracle_rate(sl, pool, cores, per)
+
+    for k in range(warmup):
+        step(k)
+    n_tot, wall_tot = 0, 0.0
+    for k in range(steps):
+        _, n, wall = step(warmup + k)
+        n_tot += n
+        wall_tot += wall
+    return n_tot / wall_tot, n_tot, wall_tot
+
+
+def ref_gpu_time(k, X: np.ndarray, steps: int, warmup: int):
+    """The reference's emd_batch_kernel on the same GPU, dense [B, N] input:
+    device-timed launches with its per-call pool allocation and fills
+    (kernels.py:1343-1372).  Returns seconds per launch."""
+    import torch
+    dev = torch.device("cuda", 0)
+    B, N = X.shape
+    sig = torch.from_numpy(np.ascontiguousarray(X)).to(dev)
+    Tn = torch.arange(N, dtype=torch.float64, device=dev)
+    k.run_device(torch.zeros((1, 64), dtype=torch.float64, device=dev), Tn[:64])  # warmup()
+    for _ in range(warmup):
+        out = k.run_device(sig, Tn)
+        del out
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        out = k.run_device(sig, Tn)
+        del out
+    e1.record(st)
+    torch.cuda.synchronize()
+    del sig
+    torch.cuda.empty_cache()
+    return e0.elapsed_time(e1) * 1e-3 / steps
+
+
 def run_reference(a, rank, world, pool, cores):
-    """The reference's own emd_batch_kernel (kernels.py:834-1080, built from
-    kernels.py into oracle/_ref by oracle/build_ref.py: CuPy is absent, so
-    nvcc stands in for its NVRTC compile) on the same GPU and workload, with
-    the reference's launch geometry and per-call pool allocation + zero-fill
-    (kernels.py:1343-1372).  The CPU oracle on the host cores is reported as
-    its cpu_baseline.  Without the built library or a GPU, the CPU oracle is
-    the measured arm."""
+    """Reference arm.  The reference's path is a CUDA kernel with no CPU
+    implementation, so its CPU arm is the oracle port (oracle/emd_oracle.py,
+    bit-identical to the reference kernel built with -fmad=false) on all host
+    cores: W untimed and K timed steps, each a bounded slice of the workload.
+    That is the line's value, its cpu_baseline and its e2e (no host<->device
+    bytes).  When oracle/_ref is built and a GPU is present, the reference's
+    own emd_batch_kernel (kernels.py:834-1080, compiled from kernels.py by
+    oracle/build_ref.py: CuPy is absent, nvcc stands in for NVRTC) on the same
+    GPU and workload is reported beside it as ``reference_gpu_kernel``, with
+    the reference's launch geometry and per-call pool allocation + fills."""
     if rank != 0:
         return
+    if a.workload == "ragged64k":
+        return run_reference_ragged(a, pool, cores)
     X = make_workload(a.workload, 0)
     B, N = X.shape
-    sample = min(a.cpu_sample or max(cores * 16, 64), B)
-    r, n, wall = cpu_oracle_rate(X, pool, cores, sample)
+    per = min(a.cpu_sample or max(cores * 8, 32), B)
+    r, n, wall = cpu_reference_steps(X, pool, cores, a.steps, a.warmup, per)
     pool.close()
     cpu = {"value": round(r, 2), "unit": "signals/s", "cores": cores, "kind": "port",
-           "sample": f"first {n} traces of the workload, NumPy oracle, {cores} processes, "
-                     f"{wall:.1f} s wall"}
+           "sample": f"{a.steps} steps of {per} traces of the workload (after {a.warmup} "
+                     f"warm-up steps), NumPy oracle, {cores} processes, {wall:.1f} s timed"}
+    line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": "signals/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(per / max(r, 1e-9) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
+                       "batch_per_gpu": B, "N": N, "parallelism": f"{cores} host processes",
+                       "step": f"{per} traces of the workload per step"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "signals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
     import torch
-    line = {"impl": "reference", "metric": METRIC, "unit": "signals/s", "n_gpus": world,
-            "steps": a.steps, "warmup": a.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "cpu_baseline": cpu}
     if os.path.isfile(REF_LIB) and torch.cuda.is_available():
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from refkernel import RefKernel
         k = RefKernel("libemd_ref.so")
         dev = torch.device("cuda", 0)
-        sig = torch.from_numpy(X).to(dev)
+        el = ref_gpu_time(k, X, a.steps, a.warmup)
         Tn = torch.arange(N, dtype=torch.float64, device=dev)
-        k.run_device(torch.zeros((1, 64), dtype=torch.float64, device=dev), Tn[:64])  # warmup()
-        for _ in range(a.warmup):
-            out = k.run_device(sig, Tn)
-            del out
-        torch.cuda.synchronize()
-        st = torch.cuda.current_stream()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(a.steps):
-            out = k.run_device(sig, Tn)
-            del out
-        e1.record(st)
-        torch.cuda.synchronize()
-        el = e0.elapsed_time(e1) * 1e-3
-        value = B * a.steps / el
         host_in = torch.from_numpy(X).pin_memory()
         host_imfs = torch.empty((B, k.max_imfs, N), dtype=torch.float64).pin_memory()
         h_n = torch.empty(B, dtype=torch.int32).pin_memory()
         h_o = torch.empty(B, dtype=torch.int32).pin_memory()
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(st)
         for _ in range(a.steps):
@@ -443,29 +493,104 @@ def run_reference(a, rank, world, pool, cores):
         e1.record(st)
         torch.cuda.synchronize()
         te = e0.elapsed_time(e1) * 1e-3
-        line.update({
-            "value": round(value, 2), "ms_per_step": round(el / a.steps * 1e3, 3),
-            "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
-                       "batch_per_gpu": B, "N": N,
-                       "reference_kernel": "emd_batch_kernel from kernels.py, nvcc -std=c++11 "
-                                           "sm_100a (oracle/_ref/libemd_ref.so); grid (batch,), "
-                                           "block 128, 57824 B dynamic smem",
-                       "parallelism": "one GPU"},
+        line["reference_gpu_kernel"] = {
+            "value": round(B / el, 2), "unit": "signals/s", "ms_per_step": round(el * 1e3, 3),
+            "kernel": "emd_batch_kernel from kernels.py, nvcc -std=c++11 sm_100a "
+                      "(oracle/_ref/libemd_ref.so); grid (batch,), block 128, 57824 B dynamic smem",
             "e2e": {"value": round(B * a.steps / te, 2), "unit": "signals/s",
                     "h2d_bytes_per_step": int(8 * B * N),
-                    "d2h_bytes_per_step": int(8 * B * k.max_imfs * N + 8 * B)},
-        })
-    else:
-        line.update({
-            "value": cpu["value"], "ms_per_step": round(B / max(r, 1e-9) * 1e3, 3),
-            "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
-                       "batch_per_gpu": B, "N": N, "parallelism": "host cores",
-                       "note": "reference kernel library not built here; CPU oracle measured"},
-            "e2e": {"value": cpu["value"], "unit": "signals/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0},
-        })
+                    "d2h_bytes_per_step": int(8 * B * k.max_imfs * N + 8 * B)}}
     print(json.dumps(line), flush=True)
 
+
+def run_reference_ragged(a, pool, cores):
+    """Reference on the ragged batch (cfg2 evaluation set).  CPU arm: the oracle
+    on bounded slices, as run_reference.  GPU reference kernel, timing only
+    (zero padding changes the decomposition): (1) the batch padded to its max
+    N = 8192, as the reference API requires one N; (2) per length bucket
+    (<=1024, 2048, 4096, 8192) padded to the bucket edge, the fairer number.
+    Both on a seeded subsample of --ref-sample traces per measurement (the
+    whole padded batch would hold ~100 GB and run for minutes); the rate of a
+    bucket scales by its trace count, so (2) is sum(bucket traces) / sum(bucket
+    traces / bucket rate)."""
+    w = WORKLOADS["ragged64k"]
+    n_eval = a.eval_traces or w["n"]
+    vals, offs = gen_ragged(pool, n_eval, w["lo"], w["hi"], seed=2)
+    lens = np.diff(offs)
+    rng = np.random.default_rng(12345)
+    per = a.cpu_sample or max(cores * 4, 32)
+    # CPU arm: the oracle over bounded random slices of the batch, all cores
+    pick = rng.permutation(n_eval)
+    rows = [vals[offs[b]:offs[b + 1]] for b in pick[: per * (a.steps + a.warmup)]]
+    t_cpu = 0.0
+    n_cpu = 0
+    for k in range(a.warmup + a.steps):
+        chunk = rows[k * per:(k + 1) * per]
+        parts = [chunk[i::cores] for i in range(cores)]
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_rows, [(p,) for p in parts if p])
+        wall = time.perf_counter() - t0
+        if k >= a.warmup:
+            t_cpu += wall
+            n_cpu += sum(r for r in res)
+    pool.close()
+    r_cpu = n_cpu / t_cpu
+    cpu = {"value": round(r_cpu, 2), "unit": "signals/s", "cores": cores, "kind": "port",
+           "sample": f"{a.steps} steps of {per} random traces of the batch (after {a.warmup} "
+                     f"warm-up steps), NumPy oracle, {cores} processes, {t_cpu:.1f} s timed"}
+    line = {"impl": "reference", "metric": "EMD signals/s (FP64) ragged batch", "value": cpu["value"],
+            "unit": "signals/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(per / max(r_cpu, 1e-9) * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": "ragged64k", "desc": w["desc"], "batch_per_gpu": n_eval,
+                       "parallelism": f"{cores} host processes"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "signals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    import torch
+    if os.path.isfile(REF_LIB) and torch.cuda.is_available():
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from refkernel import RefKernel
+        k = RefKernel("libemd_ref.so")
+        ns = a.ref_sample
+
+        def padded(idx, width):
+            P = np.zeros((idx.size, width), dtype=np.float64)
+            for r, b in enumerate(idx):
+                P[r, :lens[b]] = vals[offs[b]:offs[b + 1]]
+            return P
+
+        sub = np.sort(rng.choice(n_eval, size=min(ns, n_eval), replace=False))
+        t_pad = ref_gpu_time(k, padded(sub, int(lens.max())), 1, 1)
+        buckets = {}
+        t_weighted = 0.0
+        for lo, hi in ((0, 1024), (1024, 2048), (2048, 4096), (4096, 8192)):
+            m = np.flatnonzero((lens > lo) & (lens <= hi))
+            if m.size == 0:
+                continue
+            bs = np.sort(rng.choice(m, size=min(ns, m.size), replace=False))
+            t_b = ref_gpu_time(k, padded(bs, hi), 1, 1)
+            rate = bs.size / t_b
+            buckets[str(hi)] = {"traces": int(m.size), "sampled": int(bs.size),
+                                "signals_per_s": round(rate, 2)}
+            t_weighted += m.size / rate
+        line["reference_gpu_kernel"] = {
+            "padded_to_max_n": {"value": round(sub.size / t_pad, 2), "unit": "signals/s",
+                                "N": int(lens.max()), "sampled": int(sub.size)},
+            "per_length_bucket": {"value": round(n_eval / t_weighted, 2), "unit": "signals/s",
+                                  "buckets": buckets},
+            "note": "timing only: zero padding changes the decomposition",
+            "kernel": "emd_batch_kernel from kernels.py, nvcc -std=c++11 sm_100a (oracle/_ref)"}
+    print(json.dumps(line), flush=True)
+
+
+def _oracle_rows(args):
+    rows, = args
+    sys.path.insert(0, ROOT)
+    from oracle import emd_oracle as O
+    for x in rows:
+        O.emd_signal(x, np.arange(x.shape[0], dtype=np.float64))
+    return len(rows)
 
 
 # ---------------------------------------------------------------------------
