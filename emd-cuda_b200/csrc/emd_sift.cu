@@ -309,26 +309,30 @@ __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int wa
   int c0 = (warp * nch) / kWarps, c1 = ((warp + 1) * nch) / kWarps;
   int rmax = 0, rmin = 0, zc = 0, zre = 0;
   bool trig = false;
+  // neighbours straight from shared memory (conflict-free consecutive
+  // doubles): no shuffles, no divergent edge loads; iterations independent
+#pragma unroll 2
   for (int c = c0; c < c1; ++c) {
     int i = (c << 5) + lane;
     double v = (i < N) ? imf[i] : 0.0;
-    double vp = __shfl_up_sync(kFull, v, 1);
-    double vn = __shfl_down_sync(kFull, v, 1);
-    if (lane == 0) vp = (i >= 1 && i - 1 < N) ? imf[i - 1] : 0.0;
-    if (lane == 31) vn = (i + 1 < N) ? imf[i + 1] : 0.0;
+    double vp = (i >= 1 && i - 1 < N) ? imf[i - 1] : 0.0;
+    double vn = (i + 1 < N) ? imf[i + 1] : 0.0;
     bool interior = (i >= 1) && (i <= N - 2);
     double dp = v - vp, dn = vn - v;
     bool strict = interior && (dp * dn < 0.0);
     bool ismin = strict && (dp < 0.0);
     bool ismax = strict && !(dp < 0.0);
-    if (interior && dn == 0.0 && dp != 0.0) {
-      // true left edge of a flat run: classify by the slopes around the run
-      int j = i;
-      while (j + 1 < N && imf[j + 1] == v) ++j;
-      if (j + 1 < N) {
-        double da = imf[j + 1] - imf[j];
-        if (dp > 0.0 && da < 0.0) ismax = true;
-        else if (dp < 0.0 && da > 0.0) ismin = true;
+    const bool flat = interior && dn == 0.0 && dp != 0.0;
+    if (__any_sync(kFull, flat)) {
+      // rare: true left edge of a flat run, classified by the slopes around it
+      if (flat) {
+        int j = i;
+        while (j + 1 < N && imf[j + 1] == v) ++j;
+        if (j + 1 < N) {
+          double da = imf[j + 1] - imf[j];
+          if (dp > 0.0 && da < 0.0) ismax = true;
+          else if (dp < 0.0 && da > 0.0) ismin = true;
+        }
       }
     }
     trig |= interior && (dp == 0.0 || dn == 0.0 || v == 0.0);
@@ -437,30 +441,9 @@ __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots
   int c0 = (warp * nch) / kWarps, c1 = ((warp + 1) * nch) / kWarps;
   unsigned lt = (1u << lane) - 1u;
   bool bad = false;
-  for (int c = c0; c < c1; ++c) {
-    uint32_t bm = L.mmax[c], bn = L.mmin[c];
-    bool ismax = (bm >> lane) & 1u, ismin = (bn >> lane) & 1u;
-    // after the ranks below are taken, the chunk's prefix becomes global
-    // (warp offset added) for the evaluation pass's segment counts
-    const int pm = L.pmax[c], pn = L.pmin[c];
-    __syncwarp();
-    if (lane == 0) {
-      L.pmax[c] = (uint16_t)(pm + e.off_max);
-      L.pmin[c] = (uint16_t)(pn + e.off_min);
-    }
-    if (!(ismax || ismin)) continue;
-    int i = (c << 5) + lane;
-    int ii = i;
-    double v = imf[i];
-    if (e.trig) {
-      double dp = v - imf[i - 1], dn = imf[i + 1] - v;
-      if (!(dp * dn < 0.0)) {       // plateau extremum: report the run's midpoint
-        int j = i;
-        while (j + 1 < N && imf[j + 1] == v) ++j;
-        ii = (i + j) / 2;
-        v = imf[ii];
-      }
-    }
+  // one extremum lane: rank it, write its knot, note head / tail indices
+  auto put = [&](uint32_t bm, uint32_t bn, int pm, int pn, int ii, double v) {
+    const bool ismax = (bm >> lane) & 1u;
     int q = ismax ? 0 : 1;
     int rank = q == 0 ? e.off_max + pm + __popc(bm & lt)
                       : e.off_min + pn + __popc(bn & lt);
@@ -475,6 +458,42 @@ __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots
       int fe = nq - 1 - rank;
       if (fe <= NB) C.tail[q][fe] = ii;
     }
+  };
+  if (!e.trig) {
+    // no exact zeros or flat runs in this proto-IMF: every extremum is strict
+#pragma unroll 2
+    for (int c = c0; c < c1; ++c) {
+      const uint32_t bm = L.mmax[c], bn = L.mmin[c];
+      const int pm = L.pmax[c], pn = L.pmin[c];
+      if (((bm | bn) >> lane) & 1u) {
+        const int i = (c << 5) + lane;
+        put(bm, bn, pm, pn, i, imf[i]);
+      }
+    }
+  } else {
+    for (int c = c0; c < c1; ++c) {
+      const uint32_t bm = L.mmax[c], bn = L.mmin[c];
+      const int pm = L.pmax[c], pn = L.pmin[c];
+      if (!(((bm | bn) >> lane) & 1u)) continue;
+      int i = (c << 5) + lane;
+      int ii = i;
+      double v = imf[i];
+      double dp = v - imf[i - 1], dn = imf[i + 1] - v;
+      if (!(dp * dn < 0.0)) {       // plateau extremum: report the run's midpoint
+        int j = i;
+        while (j + 1 < N && imf[j + 1] == v) ++j;
+        ii = (i + j) / 2;
+        v = imf[ii];
+      }
+      put(bm, bn, pm, pn, ii, v);
+    }
+  }
+  // the chunks' prefixes become global (warp offset added) for the evaluation
+  // pass's segment counts, once every lane has taken its ranks
+  __syncwarp();
+  for (int c = c0 + lane; c < c1; c += 32) {
+    L.pmax[c] = (uint16_t)(L.pmax[c] + e.off_max);
+    L.pmin[c] = (uint16_t)(L.pmin[c] + e.off_min);
   }
   return bad;
 }
