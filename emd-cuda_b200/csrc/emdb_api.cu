@@ -36,6 +36,15 @@ struct emdb_plan {
   unsigned* d_chunk_count = nullptr;
   unsigned* h_chunk_flag = nullptr;   // pinned, mapped
   unsigned* d_chunk_flag = nullptr;   // its device alias
+  // input groups: each group of traces is its own launch on its own stream,
+  // with its own queue ticket and slab region, started once its input is in
+  static constexpr int kGroups = 4;
+  cudaStream_t group_stream[kGroups] = {};
+  cudaEvent_t ev_in[kGroups] = {};
+  cudaEvent_t ev_group[kGroups] = {};
+  int* d_group_queue = nullptr;
+  char* d_group_slab = nullptr;
+  size_t group_slab_bytes = 0;
   std::mutex mu;
 };
 
@@ -123,7 +132,9 @@ int check_config(const emdb_config* c) {
   return EMDB_OK;
 }
 
-int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st) {
+// Arena, occupancy and the launch-independent SiftParams fields; *grid = the
+// persistent grid for sp.batch traces.
+int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
   int arena = arena_for(p, max_n);
   if (arena <= 0 || emdb::sift_fixed_smem(max_n) + 64 > (size_t)arena)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
@@ -132,21 +143,28 @@ int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st
   cudaError_t e = emdb::sift_occupancy(arena, p->variant, &per_sm);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
-  int grid = std::min(sp.batch, per_sm * p->num_sms);
+  *grid = std::min(sp.batch, per_sm * p->num_sms);
   sp.variant = p->variant;
-  int rc = ensure_slab(p, grid);
-  if (rc) return rc;
-  sp.queue = p->d_ctl;
   sp.status = p->d_ctl + 1;
   sp.counters = p->d_cnt;
-  sp.slab = p->d_slab;
   sp.slab_stride = p->slab_stride;
   sp.arena_bytes = arena;
   sp.max_extrema = p->cfg.max_extrema;
   sp.nbsym = p->cfg.nbsym;
   sp.max_iteration = p->cfg.max_iteration;
   sp.max_imfs = p->cfg.max_imfs;
-  e = cudaMemsetAsync(p->d_ctl, 0, sizeof(int), st);
+  return EMDB_OK;
+}
+
+int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st) {
+  int grid = 0;
+  int rc = prepare_sift(p, sp, max_n, &grid);
+  if (rc) return rc;
+  rc = ensure_slab(p, grid);
+  if (rc) return rc;
+  sp.queue = p->d_ctl;
+  sp.slab = p->d_slab;
+  cudaError_t e = cudaMemsetAsync(p->d_ctl, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_fail(e, "queue reset");
   e = emdb::launch_sift(sp, grid, st);
   if (e != cudaSuccess) return cuda_fail(e, "sift launch");
@@ -212,6 +230,13 @@ int emdb_plan_destroy(emdb_plan* p) {
     if (p->h_chunk_flag) cudaFreeHost(p->h_chunk_flag);
     if (p->ev_kernel) cudaEventDestroy(p->ev_kernel);
     if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+    for (int g = 0; g < emdb_plan::kGroups; ++g) {
+      if (p->group_stream[g]) cudaStreamDestroy(p->group_stream[g]);
+      if (p->ev_in[g]) cudaEventDestroy(p->ev_in[g]);
+      if (p->ev_group[g]) cudaEventDestroy(p->ev_group[g]);
+    }
+    if (p->d_group_queue) cudaFree(p->d_group_queue);
+    if (p->d_group_slab) cudaFree(p->d_group_slab);
   }
   delete p;
   return EMDB_OK;
@@ -311,18 +336,28 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     p->stage_bytes = total;
   }
   constexpr int kMaxChunks = 256;
+  constexpr int kG = emdb_plan::kGroups;
   if (!p->copy_stream) {
     e = cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_kernel, cudaEventDisableTiming);
+    for (int k = 0; k < kG && e == cudaSuccess; ++k) {
+      e = cudaStreamCreateWithFlags(&p->group_stream[k], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_in[k], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_group[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_group_queue, kG * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_chunk_count, kMaxChunks * sizeof(unsigned));
     if (e == cudaSuccess)
       e = cudaHostAlloc(&p->h_chunk_flag, kMaxChunks * sizeof(unsigned), cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->d_chunk_flag, p->h_chunk_flag, 0);
     if (e != cudaSuccess) return cuda_fail(e, "setting up the host pipeline");
   }
-  // chunks of >= 64 traces, at most kMaxChunks of them
+  // chunks of >= 64 traces, at most kMaxChunks of them; groups are whole
+  // chunks (4 groups for large batches, so the first launch starts after a
+  // quarter of the input copy)
   const int chunk = std::max(64, (batch + kMaxChunks - 1) / kMaxChunks);
   const int nchunk = (batch + chunk - 1) / chunk;
+  const int ngroup = nchunk >= 4 * kG ? kG : 1;
   volatile unsigned* flag = p->h_chunk_flag;
   // the previous call on this plan has returned, so no kernel writes the flags now
   for (int c = 0; c < nchunk; ++c) flag[c] = 0u;
@@ -336,37 +371,87 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   int* d_dn = reinterpret_cast<int*>(d + o_dbg);
   int* d_de = reinterpret_cast<int*>(d + o_dbg + al(dbg_bytes));
   int* d_dz = reinterpret_cast<int*>(d + o_dbg + 2 * al(dbg_bytes));
-  e = cudaMemsetAsync(p->d_chunk_count, 0, nchunk * sizeof(unsigned), st);
-  if (e == cudaSuccess && N > 0)
-    e = cudaMemcpyAsync(d_sig, signals, B * n * 8, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && T) e = cudaMemcpyAsync(d_T, T, n * 8, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return cuda_fail(e, "host-pipeline input copy");
 
-  emdb::SiftParams sp{};
-  sp.values = d_sig;
-  sp.offsets = nullptr;
-  sp.dense_n = N;
-  sp.T = d_T;
-  sp.t_mode = T ? emdb::kTShared : emdb::kTArange;
-  sp.batch = batch;
-  sp.order = nullptr;
-  sp.imfs = d_imf;
-  sp.n_imfs = d_n;
-  sp.overflow = d_ov;
-  sp.dbg_n = d_dn;
-  sp.dbg_ext = d_de;
-  sp.dbg_nzm = d_dz;
-  sp.chunk_count = p->d_chunk_count;
-  sp.chunk_flag = p->d_chunk_flag;
-  sp.chunk_traces = chunk;
-  int rc = launch_common(p, sp, N, st);
-  if (rc) return rc;
-  e = cudaEventRecord(p->ev_kernel, st);
-  if (e != cudaSuccess) return cuda_fail(e, "host-pipeline event");
+  // launch-independent parameters and the per-group grid
+  emdb::SiftParams base{};
+  base.offsets = nullptr;
+  base.dense_n = N;
+  base.T = d_T;
+  base.t_mode = T ? emdb::kTShared : emdb::kTArange;
+  base.order = nullptr;
+  base.chunk_flag = p->d_chunk_flag;
+  base.chunk_traces = chunk;
+  int gchunks[kG], gstart[kG], gcount[kG], grid[kG];
+  for (int k = 0, c = 0; k < ngroup; ++k) {
+    gchunks[k] = nchunk / ngroup + (k < nchunk % ngroup ? 1 : 0);
+    gstart[k] = c * chunk;
+    gcount[k] = std::min(batch, (c + gchunks[k]) * chunk) - gstart[k];
+    c += gchunks[k];
+    emdb::SiftParams sp = base;
+    sp.batch = gcount[k];
+    int rc = prepare_sift(p, sp, N, &grid[k]);
+    if (rc) return rc;
+    if (k == 0) base = sp;                     // arena and config fields are shared
+  }
+  size_t slab_need = 0;
+  for (int k = 0; k < ngroup; ++k) slab_need += (size_t)grid[k] * p->slab_stride;
+  if (slab_need > p->group_slab_bytes) {
+    if (p->d_group_slab) cudaFree(p->d_group_slab);
+    p->d_group_slab = nullptr;
+    p->group_slab_bytes = 0;
+    e = cudaMalloc(&p->d_group_slab, slab_need);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating host-pipeline spill slabs");
+    p->group_slab_bytes = slab_need;
+  }
+
+  // inputs group by group on the caller's stream; each group launches on its
+  // own stream once its traces are in
+  e = cudaMemsetAsync(p->d_chunk_count, 0, nchunk * sizeof(unsigned), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->d_group_queue, 0, kG * sizeof(int), st);
+  if (e == cudaSuccess && T) e = cudaMemcpyAsync(d_T, T, n * 8, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(e, "host-pipeline set-up");
+  // on a failure after the first launch, let what was issued finish before
+  // returning: the staging and slabs are reused by the next call
+  auto drain = [&](cudaError_t err, const char* what) {
+    for (int k = 0; k < ngroup; ++k) cudaStreamSynchronize(p->group_stream[k]);
+    cudaStreamSynchronize(st);
+    return cuda_fail(err, what);
+  };
+  size_t slab_off = 0;
+  for (int k = 0; k < ngroup; ++k) {
+    const size_t t0 = (size_t)gstart[k], cnt = (size_t)gcount[k];
+    if (N > 0)
+      e = cudaMemcpyAsync(d_sig + t0 * n, signals + t0 * n, cnt * n * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(p->ev_in[k], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(p->group_stream[k], p->ev_in[k], 0);
+    if (e != cudaSuccess) return drain(e, "host-pipeline input copy");
+    emdb::SiftParams sp = base;
+    sp.values = d_sig + t0 * n;
+    sp.batch = (int)cnt;
+    sp.imfs = d_imf + t0 * (size_t)mi * n;
+    sp.n_imfs = d_n + t0;
+    sp.overflow = d_ov + t0;
+    sp.dbg_n = d_dn + t0 * mi;
+    sp.dbg_ext = d_de + t0 * mi;
+    sp.dbg_nzm = d_dz + t0 * mi;
+    sp.queue = p->d_group_queue + k;
+    sp.slab = p->d_group_slab + slab_off;
+    sp.chunk_count = p->d_chunk_count + gstart[k] / chunk;
+    sp.chunk_flag = p->d_chunk_flag + gstart[k] / chunk;
+    slab_off += (size_t)grid[k] * p->slab_stride;
+    e = emdb::launch_sift(sp, grid[k], p->group_stream[k]);
+    if (e == cudaSuccess) e = cudaEventRecord(p->ev_group[k], p->group_stream[k]);
+    if (e != cudaSuccess) return drain(e, "sift launch");
+  }
+  // only now does the caller's stream wait for the kernels: waiting inside the
+  // loop would hold the next group's input copy behind this group's kernel
+  for (int k = 0; k < ngroup && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(st, p->ev_group[k], 0);
+  if (e == cudaSuccess) e = cudaEventRecord(p->ev_kernel, st);     // after every group's kernel
+  if (e != cudaSuccess) return drain(e, "host-pipeline event");
 
   // Copy each chunk's IMF rows back as soon as its flag is up.  Once the
-  // kernel has finished every remaining chunk is copied, so this loop ends
-  // with the kernel whatever the flags say.
+  // kernels have finished every remaining chunk is copied, so this loop ends
+  // with them whatever the flags say.
   const size_t row_bytes = (size_t)mi * n * 8;
   std::string err;
   std::vector<char> done(nchunk, 0);
@@ -396,12 +481,12 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
       }
       if (e != cudaErrorNotReady) {
         cudaStreamSynchronize(p->copy_stream);
-        return cuda_fail(e, "sift kernel");
+        return drain(e, "sift kernel");
       }
     }
     if (!moved) std::this_thread::sleep_for(std::chrono::microseconds(20));
   }
-  // per-trace counts and debug rows after the whole kernel
+  // per-trace counts and debug rows after every kernel
   e = cudaStreamWaitEvent(p->copy_stream, p->ev_kernel, 0);
   if (e == cudaSuccess) e = cudaMemcpyAsync(n_imfs, d_n, B * 4, cudaMemcpyDeviceToHost, p->copy_stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(overflow, d_ov, B * 4, cudaMemcpyDeviceToHost, p->copy_stream);

@@ -40,17 +40,18 @@ def test_host_numpy_equals_device(batch, N):
 
 
 @pytest.mark.gpu
-def test_host_with_time_axis_and_out_buffers():
+@pytest.mark.parametrize("batch", [300, 2000])      # one launch; four input groups
+def test_host_with_time_axis_and_out_buffers(batch):
     emd = GPUBatchEMD()
     rng = np.random.default_rng(11)
-    X = W.sinusoid_batch(300, 700, seed=4)
+    X = W.sinusoid_batch(batch, 700, seed=4)
     T = np.cumsum(rng.uniform(0.5, 1.5, 700))
     ref = _device(emd, X, T)
     xin = torch.from_numpy(X).pin_memory()
     mi = emd.config.max_imfs
-    out = (torch.full((300, mi, 700), np.nan, dtype=torch.float64).pin_memory(),
-           torch.full((300,), -7, dtype=torch.int32).pin_memory(),
-           torch.full((300,), -7, dtype=torch.int32).pin_memory())
+    out = (torch.full((batch, mi, 700), np.nan, dtype=torch.float64).pin_memory(),
+           torch.full((batch,), -7, dtype=torch.int32).pin_memory(),
+           torch.full((batch,), -7, dtype=torch.int32).pin_memory())
     imfs, n, o = emd(xin, T=T, out=out)
     assert imfs.data_ptr() == out[0].data_ptr()
     _same((imfs.numpy(), n.numpy(), o.numpy()) + tuple(x.numpy() for x in emd.last_debug), ref)
