@@ -51,11 +51,12 @@
 // raise register pressure more than they add overlap; EMDB_FAST_DIV 0/1/2/3
 // ran at 142.5k/154.3k/150.8k/154.9k signals/s, bit-identical outputs.  The
 // gain is the straight-line evaluation: every hardware division carries its
-// own slow-path branch, which splits the sample's independent chains.  A
-// branch-free division with no reciprocal at hand (approximate reciprocal,
-// two Newton steps, a Markstein correction and an exact-remainder choice of
-// neighbour) in the PCR rows and the remaining quotients ran slower: 160k vs
-// 180k signals/s -- more instructions than the overlap it buys.
+// own slow-path branch, which splits the sample's independent chains.
+//  EMDB_PCR_NB     branch-free division with no reciprocal at hand (div_nb)
+//                  for the two PCR quotients of each row: 241.1k vs 222.8k
+//                  signals/s on one B200.  Used everywhere (evaluation and
+//                  stop-test quotients too) it ran slower, 160k vs 180k: there
+//                  the extra instructions outweigh the overlap.
 #ifndef EMDB_EVAL_PAIR
 #define EMDB_EVAL_PAIR 0
 #endif
@@ -70,6 +71,9 @@
 #endif
 #ifndef EMDB_TREE_SPLIT
 #define EMDB_TREE_SPLIT 1
+#endif
+#ifndef EMDB_PCR_NB
+#define EMDB_PCR_NB 1
 #endif
 
 namespace emdb {
@@ -285,6 +289,39 @@ __device__ __forceinline__ double div_q(double a, double b, double y, bool& slow
   slow |= !(zero || (aa > 0x1p-900 && aa < 0x1p+900 && qa > 0x1p-900 && qa < 0x1p+900));
   return zero ? q0 : q2;
 }
+
+#if EMDB_PCR_NB
+// Branch-free RN(a/b) with no reciprocal at hand (FMA division schemes in
+// Muller et al., "Handbook of Floating-Point Arithmetic", 2nd ed., ch. 4.9 /
+// 5.3): y ~ 1/b from the PTX approximate reciprocal and two Newton steps;
+// q1 = q0 + (a - b*q0)*y is a faithful rounding of a/b; the exact remainders
+// of q1 and of its neighbour towards a/b pick the nearer one (a quotient of
+// two 53-bit numbers is never an exact midpoint).  `slow` is set outside the
+// ranges where every step is exact: |a|, |q| in (2^-900, 2^900), |b| in
+// (2^-1000, 2^1000); zero numerators only with such a b.
+__device__ __forceinline__ double div_nb(double a, double b, bool& slow) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  const double q0 = a * y;
+  const double r0 = fma(-q0, b, a);
+  const double q1 = fma(r0, y, q0);
+  const double r1 = fma(-q1, b, a);
+  const bool up = (r1 > 0.0) == (b > 0.0);
+  const long long step = (up == (q1 > 0.0)) ? 1 : -1;
+  const double qn = __longlong_as_double(__double_as_longlong(q1) + step);
+  const double rn = fma(-qn, b, a);
+  const double q = fabs(rn) < fabs(r1) ? qn : q1;
+  const double aa = fabs(a), qa = fabs(q1), ba = fabs(b);
+  const bool bok = ba > 0x1p-1000 && ba < 0x1p+1000;
+  const bool zero = a == 0.0;
+  slow |= !bok || (!zero && !(aa > 0x1p-900 && aa < 0x1p+900 && qa > 0x1p-900 && qa < 0x1p+900));
+  return zero ? q0 : q;
+}
+#endif
 
 __device__ __forceinline__ double div_rn(double a, double b, double y) {
   bool slow = false;
@@ -659,8 +696,20 @@ __device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* _
   const double ak = Pa[r], bk = Pa[cap + r], ck = Pa[2 * cap + r], dk = Pa[3 * cap + r];
   const double b_left = hl ? Pa[cap + rl] : 1.0;
   const double b_right = hr ? Pa[cap + rr] : 1.0;
+#if EMDB_PCR_NB
+  bool sl = false, sr = false;
+  const double ql = div_nb(ak, b_left, sl);
+  const double qr = div_nb(ck, b_right, sr);
+  double alpha = hl ? ql : 0.0;
+  double beta = hr ? qr : 0.0;
+  if ((hl && sl) || (hr && sr)) {
+    alpha = hl ? ak / b_left : 0.0;
+    beta = hr ? ck / b_right : 0.0;
+  }
+#else
   const double alpha = hl ? ak / b_left : 0.0;
   const double beta = hr ? ck / b_right : 0.0;
+#endif
   const double a_left = hl ? Pa[rl] : 0.0;
   const double c_left = hl ? Pa[2 * cap + rl] : 0.0;
   const double d_left = hl ? Pa[3 * cap + rl] : 0.0;
@@ -1453,6 +1502,38 @@ __global__ void div_check_kernel(int mode, long long n, unsigned long long seed,
         if (__double_as_longlong(div_rn(a, b, y)) != __double_as_longlong(a / b)) ++bad0;
       }
     }
+#if EMDB_PCR_NB
+  } else if (mode == 2) {
+    // div_nb: [0] random a/b over [2^-1100, 2^1100] (zeros, subnormals, infinities
+    // through the fallback), [1] all-ones / power-of-two significands of b,
+    // [2] PCR-like |a| <= |b| within 2^+-40 of 1
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+      uint64_t h1 = mix64(seed ^ (uint64_t)i), h2 = mix64(h1 ^ 0x5bd1e995ull);
+      double ma = __longlong_as_double((long long)((h1 >> 12) | 0x3ff0000000000000ull));
+      double mb = __longlong_as_double((long long)((h2 >> 12) | 0x3ff0000000000000ull));
+      double a = ldexp(ma, (int)(h1 % 2201) - 1100), b = ldexp(mb, (int)(h2 % 2201) - 1100);
+      if (h1 & 1) a = -a;
+      if (h2 & 2) b = -b;
+      bool slow = false;
+      double q = div_nb(a, b, slow);
+      if (slow) q = div_slow(a, b);
+      if (__double_as_longlong(q) != __double_as_longlong(div_slow(a, b))) ++bad0;
+      const int eb2 = (int)((h2 >> 20) % 161) - 80;
+      double b2 = (h2 & 4) ? ldexp(__longlong_as_double(0x3fffffffffffffffll), eb2) : ldexp(1.0, eb2);
+      if (h2 & 8) b2 = -b2;
+      slow = false;
+      q = div_nb(a, b2, slow);
+      if (slow) q = div_slow(a, b2);
+      if (__double_as_longlong(q) != __double_as_longlong(div_slow(a, b2))) ++bad1;
+      double b3 = ldexp(mb, (int)((h2 >> 30) % 81) - 40);
+      double a3 = b3 * ((double)((h1 >> 11) & 0xfffffffffffffull) * 0x1p-52);
+      if (h1 & 16) a3 = -a3;
+      slow = false;
+      q = div_nb(a3, b3, slow);
+      if (slow) q = div_slow(a3, b3);
+      if (__double_as_longlong(q) != __double_as_longlong(div_slow(a3, b3))) ++bad2;
+    }
+#endif
   } else {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
       uint64_t h1 = mix64(seed ^ (uint64_t)i), h2 = mix64(h1 ^ 0x5bd1e995ull);

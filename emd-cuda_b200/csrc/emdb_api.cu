@@ -604,7 +604,7 @@ __attribute__((visibility("hidden"))) int emdb_noalloc_fail(int code, const char
 
 int emdb_check_division(int mode, long long n, unsigned long long seed,
                         unsigned long long* mismatches) {
-  if (!mismatches || (mode != 0 && mode != 1) || n < 0)
+  if (!mismatches || mode < 0 || mode > 2 || n < 0)
     return fail(EMDB_ERR_INVALID, "bad self-test arguments");
   unsigned long long* d = nullptr;
   cudaError_t e = cudaMalloc(&d, 3 * sizeof(unsigned long long));

@@ -156,8 +156,10 @@ class Plan:
 
 
 def check_division(mode: int, n: int, seed: int = 0) -> tuple[int, int, int]:
-    """Mismatches of the reciprocal-based division vs the hardware division,
-    per case: (general a/b, a/6, segment quotients).  Self-test."""
+    """Self-test: mismatches of the kernels' own divisions vs the hardware
+    division, three counters per mode (mode 0/1: the reciprocal-based
+    division of the evaluation; mode 2: the PCR rows' branch-free division;
+    the header documents the cases)."""
     L = load()
     out = (ctypes.c_ulonglong * 3)()
     check(L.emdb_check_division(int(mode), int(n), int(seed), out), "emdb_check_division")

@@ -192,7 +192,11 @@ int emdb_mlp_infer_bf16(const uint16_t* params_bf16, const float* X, const float
  * hardware IEEE division, in mismatches[3] (host array).  mode 0: every
  * integer pair 0 <= a <= b <= n (count in [0]); mode 1: n seeded random
  * cases each of [0] a/b over [2^-300, 2^300], [1] a/6, [2] a/b with
- * 0 <= a <= b, b in [1, 65537).  Synchronous on the current device. */
+ * 0 <= a <= b, b in [1, 65537).  mode 2: the branch-free division the PCR
+ * rows use (no reciprocal at hand), n seeded cases each of [0] a/b over
+ * [2^-1100, 2^1100] (zeros, subnormals and infinities through its fallback),
+ * [1] denominators with all-ones or power-of-two significands, [2] |a| <= |b|
+ * within 2^+-40 of 1.  Synchronous on the current device. */
 int emdb_check_division(int mode, long long n, unsigned long long seed,
                         unsigned long long* mismatches);
 
