@@ -57,6 +57,9 @@
 //                  signals/s on one B200.  Used everywhere (evaluation and
 //                  stop-test quotients too) it ran slower, 160k vs 180k: there
 //                  the extra instructions outweigh the overlap.
+//  EMDB_ACC_NB / EMDB_SETUP_NB  the same division for the stop-test quotient
+//                  diff/new and the spline rows' slopes: 231.0k / 236.7k vs
+//                  240.9k signals/s, so off.
 #ifndef EMDB_EVAL_PAIR
 #define EMDB_EVAL_PAIR 0
 #endif
@@ -74,6 +77,12 @@
 #endif
 #ifndef EMDB_PCR_NB
 #define EMDB_PCR_NB 1
+#endif
+#ifndef EMDB_ACC_NB
+#define EMDB_ACC_NB 0
+#endif
+#ifndef EMDB_SETUP_NB
+#define EMDB_SETUP_NB 0
 #endif
 
 namespace emdb {
@@ -290,7 +299,7 @@ __device__ __forceinline__ double div_q(double a, double b, double y, bool& slow
   return zero ? q0 : q2;
 }
 
-#if EMDB_PCR_NB
+#if EMDB_PCR_NB || EMDB_ACC_NB || EMDB_SETUP_NB
 // Branch-free RN(a/b) with no reciprocal at hand (FMA division schemes in
 // Muller et al., "Handbook of Floating-Point Arithmetic", 2nd ed., ch. 4.9 /
 // 5.3): y ~ 1/b from the PTX approximate reciprocal and two Newton steps;
@@ -685,7 +694,14 @@ __device__ __forceinline__ void setup_row(const double* x, const double* y, int 
     int i = k + 1;
     double h_im1 = x[i] - x[i - 1], h_i = x[i + 1] - x[i];
     a = h_im1; b = 2.0 * (h_im1 + h_i); c = h_i;
+#if EMDB_SETUP_NB
+    bool slow = false;
+    const double sr = div_nb(y[i + 1] - y[i], h_i, slow);
+    const double sl = div_nb(y[i] - y[i - 1], h_im1, slow);
+    d = slow ? 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1) : 6.0 * (sr - sl);
+#else
     d = 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1);
+#endif
   }
 }
 
@@ -901,7 +917,13 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
   ps.sq += nw * nw;
   ps.dsq += diff * diff;
   ps.osq += old * old;
+#if EMDB_ACC_NB
+  bool slow = false;
+  double qd = div_nb(diff, nw, slow);
+  if (slow) qd = diff / nw;
+#else
   double qd = diff / nw;
+#endif
   ps.std_ += qd * qd;
   ps.omax = fmax(ps.omax, old);
   ps.omin = fmin(ps.omin, old);
@@ -1502,7 +1524,7 @@ __global__ void div_check_kernel(int mode, long long n, unsigned long long seed,
         if (__double_as_longlong(div_rn(a, b, y)) != __double_as_longlong(a / b)) ++bad0;
       }
     }
-#if EMDB_PCR_NB
+#if EMDB_PCR_NB || EMDB_ACC_NB || EMDB_SETUP_NB
   } else if (mode == 2) {
     // div_nb: [0] random a/b over [2^-1100, 2^1100] (zeros, subnormals, infinities
     // through the fallback), [1] all-ones / power-of-two significands of b,
