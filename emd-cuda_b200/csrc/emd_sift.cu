@@ -60,6 +60,8 @@
 //  EMDB_ACC_NB / EMDB_SETUP_NB  the same division for the stop-test quotient
 //                  diff/new and the spline rows' slopes: 231.0k / 236.7k vs
 //                  240.9k signals/s, so off.
+//  EMDB_SETUP_TAB  on the integer time axis, the spline rows' slopes from the
+//                  reciprocal table and div_q: 238.0k vs 241.2k, so off.
 #ifndef EMDB_EVAL_PAIR
 #define EMDB_EVAL_PAIR 0
 #endif
@@ -83,6 +85,9 @@
 #endif
 #ifndef EMDB_SETUP_NB
 #define EMDB_SETUP_NB 0
+#endif
+#ifndef EMDB_SETUP_TAB
+#define EMDB_SETUP_TAB 0
 #endif
 
 namespace emdb {
@@ -338,6 +343,18 @@ __device__ __forceinline__ double div_rn(double a, double b, double y) {
   return slow ? div_slow(a, b) : q;
 }
 constexpr double kInv6 = 1.0 / 6.0;   // RN(1/6), folded at compile time
+
+// RN(1/h) for integer h in [1, kRcpTab], built at compile time by IEEE
+// division and shipped initialised in the module.
+constexpr int kRcpTab = 16384;
+struct RcpTab { double v[kRcpTab + 1]; };
+constexpr RcpTab make_rcp_tab() {
+  RcpTab t{};
+  for (int h = 1; h <= kRcpTab; ++h) t.v[h] = 1.0 / (double)h;
+  return t;
+}
+__device__ const RcpTab g_rcp = make_rcp_tab();
+
 
 struct TimeAxis {
   const double* T;
@@ -680,6 +697,12 @@ __device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K,
 // ---------------------------------------------------------------------------
 // Not-a-knot spline: reduced system + PCR + moments (kernels.py:607-697).
 // ---------------------------------------------------------------------------
+// kInt: integer time axis (T = arange), where knot spacings are integers and
+// the interior rows' slope quotients take RN(1/h) from the table and the exact
+// two-step Markstein quotient (div_q) instead of two divisions; spacings
+// outside the table (or not positive integers, as unsorted knot lists can
+// give) take the divisions.
+template <bool kInt = false>
 __device__ __forceinline__ void setup_row(const double* x, const double* y, int n, int k, int m,
                                           double& a, double& b, double& c, double& d) {
   if (k == 0) {
@@ -700,7 +723,17 @@ __device__ __forceinline__ void setup_row(const double* x, const double* y, int 
     const double sl = div_nb(y[i] - y[i - 1], h_im1, slow);
     d = slow ? 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1) : 6.0 * (sr - sl);
 #else
-    d = 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1);
+    if (kInt) {
+      const bool ok = h_i >= 1.0 && h_i <= (double)kRcpTab && h_im1 >= 1.0 &&
+                      h_im1 <= (double)kRcpTab;
+      const int ji = ok ? (int)h_i : 1, jm = ok ? (int)h_im1 : 1;
+      bool slow = !ok || (double)ji != h_i || (double)jm != h_im1;
+      const double sr = div_q(y[i + 1] - y[i], h_i, g_rcp.v[ji], slow);
+      const double sl = div_q(y[i] - y[i - 1], h_im1, g_rcp.v[jm], slow);
+      d = slow ? 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1) : 6.0 * (sr - sl);
+    } else {
+      d = 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1);
+    }
 #endif
   }
 }
@@ -738,6 +771,7 @@ __device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* _
   Pn[3 * cap + r] = dk - alpha * d_left - beta * d_right;
 }
 
+template <bool kInt = false>
 __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kbase1, int kcnt0,
                                               int kcnt1, int tid) {
   const int m0 = kcnt0 >= 4 ? kcnt0 - 2 : 0;
@@ -754,7 +788,7 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     const double* x = s0 ? x0b : x1b;
     const double* y = s0 ? y0b : y1b;
     double a, b, c, d;
-    setup_row(x, y, s0 ? kcnt0 : kcnt1, k, s0 ? m0 : m1, a, b, c, d);
+    setup_row<kInt>(x, y, s0 ? kcnt0 : kcnt1, k, s0 ? m0 : m1, a, b, c, d);
     double* P = K.P[0];
     P[r] = a; P[cap + r] = b; P[2 * cap + r] = c; P[3 * cap + r] = d;
   }
@@ -929,17 +963,6 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
   ps.omin = fmin(ps.omin, old);
 }
 
-// RN(1/h) for integer h in [1, kRcpTab], built at compile time by IEEE
-// division and shipped initialised in the module.
-constexpr int kRcpTab = 16384;
-struct RcpTab { double v[kRcpTab + 1]; };
-constexpr RcpTab make_rcp_tab() {
-  RcpTab t{};
-  for (int h = 1; h <= kRcpTab; ++h) t.v[h] = 1.0 / (double)h;
-  return t;
-}
-__device__ const RcpTab g_rcp = make_rcp_tab();
-
 // eval_seg for the time axis T = arange(N): knot positions (true and
 // mirrored) and sample times are integers, so A = (x1-t)/h and B = (t-x0)/h
 // are quotients of integers 0 <= a <= h.  For those, q0 = RN(a*y) with
@@ -1003,7 +1026,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   }
   ps.bad = __syncthreads_or(bad || mbad) != 0;
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
-  solve_splines(K, kb0, kb1, kn0, kn1, tid);
+  solve_splines<kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid);
   const double* oldv = kPlace == kPlaceBorrow ? borrow_save(slab) : imf;
 
   SideView sv0, sv1;
