@@ -175,8 +175,9 @@ class CostModel:
         pay the one-time launch set-up of the kernels it uses (~0.4 s measured
         on B200, against ~0.3 ms for 65,536 traces once warm)."""
         import torch
-        predicted_cost(self, torch.zeros((1, N_FEAT), dtype=torch.float32, device=self.device),
-                       torch.ones(1, dtype=torch.int64, device=self.device))
+        n = 4096    # large enough for the vectorised paths of every kernel used
+        predicted_cost(self, torch.zeros((n, N_FEAT), dtype=torch.float32, device=self.device),
+                       torch.ones(n, dtype=torch.int64, device=self.device))
         torch.cuda.synchronize(self.device)
 
     # -- persistence ---------------------------------------------------------------
@@ -203,7 +204,10 @@ def predicted_cost(model: CostModel, feats, lengths):
     """Work estimate per trace: N x predicted sift passes."""
     import torch
     y = model.predict(feats)
-    passes = torch.exp2(y[:, 0]).clamp(min=1.0) - 1.0
+    # 2^y as exp(y ln 2): torch's precompiled exp, where exp2 is compiled at run
+    # time on first use of each vector width (~0.4 s inside a timed step); the
+    # estimate only orders the queue
+    passes = torch.exp(y[:, 0] * 0.6931471805599453).clamp(min=1.0) - 1.0
     return lengths.to(torch.float32) * passes.clamp(min=1.0)
 
 
