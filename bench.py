@@ -62,10 +62,11 @@ WORKLOADS = {
 def make_workload(name: str, rank: int = 0):
     from cuda_emd import workloads as W
     w = WORKLOADS[name]
+    from cuda_emd.replicas import workload_seed
     if name.startswith("seismic"):
-        X = W.seismic_batch(w["n"], w["N"], seed=1 + 1000 * rank)
+        X = W.seismic_batch(w["n"], w["N"], seed=workload_seed(1, rank))
     else:
-        X = W.sinusoid_batch(w["n"], w["N"], seed=0 + 1000 * rank)
+        X = W.sinusoid_batch(w["n"], w["N"], seed=workload_seed(0, rank))
     return np.ascontiguousarray(X)
 
 
@@ -217,13 +218,10 @@ def main():
         return
 
     import torch
-    import torch.distributed as dist
+    from cuda_emd import replicas as R
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    R.init(world, "nccl", dev)
 
     from cuda_emd import GPUBatchEMD, EMDKernelConfig
 
@@ -254,8 +252,7 @@ def main():
     flops_per_step = algorithmic_flops(N, n_imfs, dbg_n, dbg_ext)
     hbm_bytes_per_step = 8.0 * B * N + 8.0 * B * cfg.max_imfs * N
 
-    if world > 1:
-        dist.barrier()
+    R.barrier(world)
     torch.cuda.synchronize(dev)
     clocks = ClockSampler(local, os.path.join(ROOT, "gpurun_out", f"clocks_r{rank}.csv")) \
         if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
@@ -272,17 +269,12 @@ def main():
         del out
     t_end.record(st)
     torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
+    R.barrier(world)
     clk = clocks.stop() if clocks else None
     elapsed = t_start.elapsed_time(t_end) * 1e-3
     per_launch = [e0.elapsed_time(e1) * 1e-3 for e0, e1 in ev]
-    if world > 1:
-        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-    total = B * a.steps * world
-    value = total / elapsed
+    elapsed = R.max_over_ranks(elapsed, world, dev)
+    value = R.whole_job_rate(B, a.steps, world, elapsed)
     ms_per_step = elapsed / a.steps * 1e3
     launch_s = statistics.mean(per_launch)
 
@@ -302,20 +294,15 @@ def main():
         for _ in range(max(1, min(a.warmup, 2))):
             e2e_step()
         torch.cuda.synchronize(dev)
-        if world > 1:
-            dist.barrier()
+        R.barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for _ in range(a.steps):
             e2e_step()
         e1.record(st)
         torch.cuda.synchronize(dev)
-        te = e0.elapsed_time(e1) * 1e-3
-        if world > 1:
-            t = torch.tensor([te], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
-        e2e = {"value": B * a.steps * world / te, "unit": "signals/s",
+        te = R.max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
+        e2e = {"value": R.whole_job_rate(B, a.steps, world, te), "unit": "signals/s",
                "h2d_bytes_per_step": int(8 * B * N),
                "d2h_bytes_per_step": int(8 * B * cfg.max_imfs * N + 8 * B
                                          + 3 * 4 * B * cfg.max_imfs)}
@@ -375,9 +362,7 @@ def main():
             "gpu_launches": a.steps,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    R.finish(world)
 
 
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libemd_ref.so")
