@@ -1173,26 +1173,30 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
 // ---------------------------------------------------------------------------
 // The sift kernel.
 // ---------------------------------------------------------------------------
-// kMinBlocks is the register-budget variant: the compiler fits the kernel
-// into 65536 / (128 * kMinBlocks) registers so that many CTAs can be resident.
 // Chunk completion for the host-memory pipeline (emdb_run_host): after the
-// barrier that follows every output write of trace b, thread 0 counts the
-// trace in its chunk's device counter; the CTA that completes the chunk
-// publishes it with one store to the chunk's flag in mapped host memory, so
-// the host can copy that chunk back while the rest of the batch sifts.  The
-// device fence before the count and the system fence before the flag order
-// all the chunk's output writes (from every CTA that counted) before the flag.
-__device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int tid) {
+// barrier that follows every output write of trace b, thread 0 raises its
+// chunk's row maximum to the trace's count of rows that may hold data (rows
+// beyond it are zero) and counts the trace in the chunk's device counter; the CTA that
+// completes the chunk publishes it with one store of 1 + the chunk's row
+// maximum to the chunk's flag in mapped host memory, so the host can copy just
+// those rows of that chunk back while the rest of the batch sifts.  The device
+// fence before the count and the system fence before the flag order all the
+// chunk's output writes (from every CTA that counted) before the flag.
+__device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int tid, int nim) {
   if (p.chunk_count == nullptr || tid != 0) return;
-  __threadfence();
   const int c = b / p.chunk_traces;
+  atomicMax(p.chunk_rows + c, (unsigned)max(nim, 0));
+  __threadfence();
   const unsigned need = (unsigned)min(p.chunk_traces, p.batch - c * p.chunk_traces);
   if (atomicAdd(p.chunk_count + c, 1u) + 1u == need) {
+    const unsigned rows = atomicMax(p.chunk_rows + c, 0u);
     __threadfence_system();
-    *reinterpret_cast<volatile unsigned*>(p.chunk_flag + c) = 1u;
+    *reinterpret_cast<volatile unsigned*>(p.chunk_flag + c) = 1u + rows;
   }
 }
 
+// kMinBlocks is the register-budget variant: the compiler fits the kernel
+// into 65536 / (128 * kMinBlocks) registers so that many CTAs can be resident.
 template <int kMinBlocks, bool kInt>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftParams p) {
   extern __shared__ __align__(16) char smem[];
@@ -1229,7 +1233,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         p.dbg_nzm[(int64_t)b * MAXI + k] = -1;
       }
       __syncthreads();
-      mark_trace_done(p, b, tid);
+      mark_trace_done(p, b, tid, MAXI);     // rows unwritten: the host copies them all
       continue;
     }
     SmemLayout L = carve(smem, N, p.arena_bytes);
@@ -1404,7 +1408,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
       p.dbg_nzm[(int64_t)b * MAXI + k] = C.dbg_z[k];
     }
     __syncthreads();
-    mark_trace_done(p, b, tid);
+    // rows that may hold data: n_imfs, plus the dropped trend row that a
+    // ~zero residue leaves in place (as the reference does)
+    mark_trace_done(p, b, tid, nim + ((trend && rzero) ? 1 : 0));
   }
 }
 

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -34,6 +35,7 @@ struct emdb_plan {
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_kernel = nullptr;
   unsigned* d_chunk_count = nullptr;
+  unsigned* d_chunk_rows = nullptr;   // per chunk: rows that may hold data
   unsigned* h_chunk_flag = nullptr;   // pinned, mapped
   unsigned* d_chunk_flag = nullptr;   // its device alias
   // input groups: each group of traces is its own launch on its own stream,
@@ -45,6 +47,7 @@ struct emdb_plan {
   int* d_group_queue = nullptr;
   char* d_group_slab = nullptr;
   size_t group_slab_bytes = 0;
+  unsigned long long host_h2d = 0, host_d2h = 0;   // bytes the last emdb_run_host moved
   std::mutex mu;
 };
 
@@ -131,6 +134,61 @@ int check_config(const emdb_config* c) {
                 "over 128 lanes");
   return EMDB_OK;
 }
+
+// Host threads that write the zero rows of the host pipeline's IMF output
+// (rows past each chunk's copied ones) while the GPU sifts: `count` blocks of
+// `len` bytes, `stride` apart, per job.
+class ZeroRows {
+ public:
+  explicit ZeroRows(bool on) {
+    if (!on) return;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nt = (int)std::max(1u, std::min(8u, hw > 2 ? hw / 2 : 1u));
+    for (int k = 0; k < nt; ++k) workers_.emplace_back([this] { run(); });
+  }
+  ~ZeroRows() { finish(); }
+  void add(char* base, size_t count, size_t stride, size_t len) {
+    if (workers_.empty()) {
+      for (size_t t = 0; t < count; ++t) std::memset(base + t * stride, 0, len);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      jobs_.push_back({base, count, stride, len});
+    }
+    cv_.notify_one();
+  }
+  void finish() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      closing_ = true;
+    }
+    cv_.notify_all();
+    for (auto& w : workers_) w.join();
+    workers_.clear();
+  }
+
+ private:
+  struct Job { char* base; size_t count, stride, len; };
+  void run() {
+    for (;;) {
+      Job j;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [this] { return closing_ || !jobs_.empty(); });
+        if (jobs_.empty()) return;
+        j = jobs_.back();
+        jobs_.pop_back();
+      }
+      for (size_t t = 0; t < j.count; ++t) std::memset(j.base + t * j.stride, 0, j.len);
+    }
+  }
+  std::vector<std::thread> workers_;
+  std::vector<Job> jobs_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  bool closing_ = false;
+};
 
 // Arena, occupancy and the launch-independent SiftParams fields; *grid = the
 // persistent grid for sp.batch traces.
@@ -227,6 +285,7 @@ int emdb_plan_destroy(emdb_plan* p) {
     if (p->d_cnt) cudaFree(p->d_cnt);
     if (p->d_stage) cudaFree(p->d_stage);
     if (p->d_chunk_count) cudaFree(p->d_chunk_count);
+    if (p->d_chunk_rows) cudaFree(p->d_chunk_rows);
     if (p->h_chunk_flag) cudaFreeHost(p->h_chunk_flag);
     if (p->ev_kernel) cudaEventDestroy(p->ev_kernel);
     if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
@@ -272,6 +331,14 @@ int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm,
   if (arena_bytes) *arena_bytes = arena;
   if (ctas_per_sm) *ctas_per_sm = per_sm;
   if (grid_max) *grid_max = per_sm * p->num_sms;
+  return EMDB_OK;
+}
+
+int emdb_host_bytes(emdb_plan* p, unsigned long long* h2d, unsigned long long* d2h) {
+  if (!p || !h2d || !d2h) return fail(EMDB_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  *h2d = p->host_h2d;
+  *d2h = p->host_d2h;
   return EMDB_OK;
 }
 
@@ -347,6 +414,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     }
     if (e == cudaSuccess) e = cudaMalloc(&p->d_group_queue, kG * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&p->d_chunk_count, kMaxChunks * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_chunk_rows, kMaxChunks * sizeof(unsigned));
     if (e == cudaSuccess)
       e = cudaHostAlloc(&p->h_chunk_flag, kMaxChunks * sizeof(unsigned), cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->d_chunk_flag, p->h_chunk_flag, 0);
@@ -407,9 +475,11 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   // inputs group by group on the caller's stream; each group launches on its
   // own stream once its traces are in
   e = cudaMemsetAsync(p->d_chunk_count, 0, nchunk * sizeof(unsigned), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p->d_chunk_rows, 0, nchunk * sizeof(unsigned), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(p->d_group_queue, 0, kG * sizeof(int), st);
   if (e == cudaSuccess && T) e = cudaMemcpyAsync(d_T, T, n * 8, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_fail(e, "host-pipeline set-up");
+  unsigned long long h2d = (unsigned long long)(B * n * 8 + (T ? n * 8 : 0)), d2h = 0;
   // on a failure after the first launch, let what was issued finish before
   // returning: the staging and slabs are reused by the next call
   auto drain = [&](cudaError_t err, const char* what) {
@@ -437,6 +507,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     sp.queue = p->d_group_queue + k;
     sp.slab = p->d_group_slab + slab_off;
     sp.chunk_count = p->d_chunk_count + gstart[k] / chunk;
+    sp.chunk_rows = p->d_chunk_rows + gstart[k] / chunk;
     sp.chunk_flag = p->d_chunk_flag + gstart[k] / chunk;
     slab_off += (size_t)grid[k] * p->slab_stride;
     e = emdb::launch_sift(sp, grid[k], p->group_stream[k]);
@@ -449,25 +520,37 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   if (e == cudaSuccess) e = cudaEventRecord(p->ev_kernel, st);     // after every group's kernel
   if (e != cudaSuccess) return drain(e, "host-pipeline event");
 
-  // Copy each chunk's IMF rows back as soon as its flag is up.  Once the
-  // kernels have finished every remaining chunk is copied, so this loop ends
-  // with them whatever the flags say.
-  const size_t row_bytes = (size_t)mi * n * 8;
+  // Copy each chunk back as soon as its flag is up: only its first `rows`
+  // rows per trace (the flag holds 1 + the largest count of rows that may
+  // hold data); host threads write the zero rows after them meanwhile.  Once
+  // the kernels have finished every remaining chunk is copied in full, so
+  // this loop ends with them whatever the flags say.
+  const size_t trace_bytes = (size_t)mi * n * 8, row_bytes = n * 8;
   std::string err;
   std::vector<char> done(nchunk, 0);
+  ZeroRows zero(imfs != nullptr && trace_bytes > 0);
   int left = nchunk;
   bool kernel_done = false;
   while (left > 0) {
     bool moved = false;
     for (int c = 0; c < nchunk; ++c) {
-      if (done[c] || !(kernel_done || flag[c] != 0u)) continue;
+      if (done[c]) continue;
+      const unsigned f = flag[c];
+      if (!(kernel_done || f != 0u)) continue;
       const size_t t0 = (size_t)c * chunk, cnt = std::min((size_t)chunk, B - t0);
-      if (row_bytes > 0) {
-        e = cudaMemcpyAsync(reinterpret_cast<char*>(imfs) + t0 * row_bytes,
-                            reinterpret_cast<char*>(d_imf) + t0 * row_bytes, cnt * row_bytes,
-                            cudaMemcpyDeviceToHost, p->copy_stream);
+      const size_t rows = f != 0u ? std::min((size_t)(f - 1u), (size_t)mi) : (size_t)mi;
+      char* dst = reinterpret_cast<char*>(imfs) + t0 * trace_bytes;
+      const char* src = reinterpret_cast<const char*>(d_imf) + t0 * trace_bytes;
+      if (trace_bytes > 0 && rows > 0) {
+        d2h += (unsigned long long)(cnt * rows * row_bytes);
+        e = rows == (size_t)mi
+                ? cudaMemcpyAsync(dst, src, cnt * trace_bytes, cudaMemcpyDeviceToHost, p->copy_stream)
+                : cudaMemcpy2DAsync(dst, trace_bytes, src, trace_bytes, rows * row_bytes, cnt,
+                                    cudaMemcpyDeviceToHost, p->copy_stream);
         if (e != cudaSuccess && err.empty()) err = "IMF copy-back";
       }
+      if (trace_bytes > 0 && rows < (size_t)mi)
+        zero.add(dst + rows * row_bytes, cnt, trace_bytes, ((size_t)mi - rows) * row_bytes);
       done[c] = 1;
       --left;
       moved = true;
@@ -494,6 +577,9 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   if (e == cudaSuccess) e = cudaMemcpyAsync(dbg_extno, d_de, dbg_bytes, cudaMemcpyDeviceToHost, p->copy_stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dbg_nzm, d_dz, dbg_bytes, cudaMemcpyDeviceToHost, p->copy_stream);
   cudaError_t e2 = cudaStreamSynchronize(p->copy_stream);
+  zero.finish();
+  p->host_h2d = h2d;
+  p->host_d2h = d2h + (unsigned long long)(2 * B * 4 + 3 * dbg_bytes);
   if (e != cudaSuccess) return cuda_fail(e, "host-pipeline result copy");
   if (e2 != cudaSuccess) return cuda_fail(e2, "host-pipeline copy stream");
   if (!err.empty()) return fail(EMDB_ERR_CUDA, err);

@@ -46,7 +46,8 @@ struct SiftParams {
   // chunk completion for copying finished traces back early (NULL = off):
   // traces [c*chunk_traces, (c+1)*chunk_traces) form chunk c
   unsigned* chunk_count;      // device counters, zeroed before launch
-  unsigned* chunk_flag;       // mapped host flags, set to 1 when chunk c is complete
+  unsigned* chunk_rows;       // device: the chunk's largest n_imfs, zeroed before launch
+  unsigned* chunk_flag;       // mapped host flags: 1 + rows to copy once chunk c is complete
   int chunk_traces;
   // config (EMDKernelConfig fields)
   int max_extrema;

@@ -28,7 +28,8 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
-           "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena")
+           "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena",
+           "emdb_host_bytes")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -64,6 +65,8 @@ def load() -> ctypes.CDLL:
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_min_arena.argtypes = [I, ctypes.POINTER(I)]
+        L.emdb_host_bytes.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
+                                      ctypes.POINTER(ctypes.c_ulonglong)]
         L.emdb_run_ragged.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]
         L.emdb_envelope.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
         L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
@@ -135,6 +138,13 @@ class Plan:
         check(self.L.emdb_plan_query(self.handle, int(max_n), ctypes.byref(a), ctypes.byref(c),
                                      ctypes.byref(g)), "emdb_plan_query")
         return a.value, c.value, g.value
+
+    def host_bytes(self) -> tuple[int, int]:
+        """(host->device, device->host) bytes of the last host-pipeline call."""
+        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        check(self.L.emdb_host_bytes(self.handle, ctypes.byref(a), ctypes.byref(b)),
+              "emdb_host_bytes")
+        return a.value, b.value
 
     def min_arena(self, max_n: int) -> int:
         """Smallest arena that holds a trace of max_n samples (knots all spilled)."""

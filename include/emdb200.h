@@ -94,13 +94,20 @@ int emdb_run(emdb_plan* plan, const double* signals, const double* T, int batch,
  * copy-back to the caller).  Inputs go up on `stream`, one sift launch covers
  * the batch, and the IMF rows of each finished chunk of traces come back on
  * the plan's own copy stream while the rest still sifts; counts and debug
- * rows follow the kernel.  Returns once every output is in host memory.
+ * rows follow the kernel; of the IMF rows only those that may hold data are
+ * copied, the zero rows after them are written by host threads meanwhile.
+ * Returns once every output is in host memory.
  * Page-locked host buffers make the copies asynchronous; pageable ones work
  * but serialise them.  Device staging (inputs + outputs) is plan-owned and
  * grows to the largest batch seen. */
 int emdb_run_host(emdb_plan* plan, const double* signals, const double* T, int batch, int N,
                   double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                   int* dbg_nzm, void* stream);
+/* Bytes the plan's last emdb_run_host copied host->device and device->host.
+ * Of each finished chunk of traces only the rows that may hold data cross
+ * the link (the kernel reports the chunk's largest count); the zero rows
+ * after them are written on the host.  No reference counterpart. */
+int emdb_host_bytes(emdb_plan* plan, unsigned long long* h2d, unsigned long long* d2h);
 
 /* CSR batch of mixed lengths in one launch: trace b is
  * values[offsets[b] .. offsets[b+1]), offsets is a DEVICE int64 [batch+1]

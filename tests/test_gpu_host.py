@@ -65,3 +65,39 @@ def test_host_rejects_bad_out():
         emd(X, out=(np.zeros((8, 3, 100)), np.zeros(8, np.int32), np.zeros(8, np.int32)))
     with pytest.raises(ValueError):
         emd(torch.from_numpy(X).cuda(), out=(None, None, None))
+
+
+@pytest.mark.gpu
+def test_host_edge_signals_equal_device():
+    """Signals whose outputs end oddly -- a pure tone (residue dropped), a
+    trend alone, a tone over a trend, all zeros, an overflowing chirp -- over
+    several chunks: the host path copies only the rows that may hold data
+    (including the dropped trend row a ~zero residue leaves in place) and
+    writes the rest as zeros; every element must equal the device path."""
+    emd = GPUBatchEMD()
+    N = 512
+    t = np.arange(N, dtype=np.float64)
+    kinds = [np.sin(2 * np.pi * t / 64.0),
+             1e-3 * t - 0.2,
+             np.sin(2 * np.pi * t / 40.0) + 2e-3 * t,
+             np.zeros(N),
+             np.sin(2 * np.pi * (0.001 + 0.2 * t / N) * t),
+             np.cos(2 * np.pi * t / 128.0) * np.exp(-t / 300.0)]
+    X = np.stack([kinds[i % len(kinds)] * (1.0 + 0.01 * (i // len(kinds))) for i in range(600)])
+    ref = _device(emd, X)
+    imfs, n, o = emd(X)
+    _same((imfs, n, o) + tuple(emd.last_debug), ref)
+
+
+@pytest.mark.gpu
+def test_host_bytes_reported():
+    """emdb_host_bytes: the inputs up, and at most the dense outputs down
+    (only rows that may hold data cross the link)."""
+    emd = GPUBatchEMD()
+    X = W.seismic_batch(512, 1024, seed=9)
+    emd(X)
+    h2d, d2h = emd._get_launcher()._plan.host_bytes()
+    mi = emd.config.max_imfs
+    dense = 512 * mi * 1024 * 8 + 2 * 512 * 4 + 3 * 512 * mi * 4
+    assert h2d == 512 * 1024 * 8
+    assert 0 < d2h <= dense
