@@ -704,6 +704,21 @@ int emdb_check_division(int mode, long long n, unsigned long long seed,
   return EMDB_OK;
 }
 
+int emdb_host_register(void* ptr, size_t bytes, int read_only) {
+  if (!ptr || bytes == 0) return fail(EMDB_ERR_INVALID, "empty host range");
+  unsigned flags = cudaHostRegisterPortable | (read_only ? cudaHostRegisterReadOnly : 0u);
+  cudaError_t e = cudaHostRegister(ptr, bytes, flags);
+  if (e != cudaSuccess) return cuda_fail(e, "page-locking the host range");
+  return EMDB_OK;
+}
+
+int emdb_host_unregister(void* ptr) {
+  if (!ptr) return fail(EMDB_ERR_INVALID, "NULL pointer");
+  cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) return cuda_fail(e, "releasing the host range");
+  return EMDB_OK;
+}
+
 int emdb_status(emdb_plan* p, int* status, void* stream) {
   if (!p || !status) return fail(EMDB_ERR_INVALID, "NULL argument");
   std::lock_guard<std::mutex> lk(p->mu);

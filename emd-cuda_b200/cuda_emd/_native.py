@@ -29,7 +29,7 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
            "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena",
-           "emdb_host_bytes")
+           "emdb_host_bytes", "emdb_host_register", "emdb_host_unregister")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -65,6 +65,8 @@ def load() -> ctypes.CDLL:
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_min_arena.argtypes = [I, ctypes.POINTER(I)]
+        L.emdb_host_register.argtypes = [VP, ctypes.c_size_t, I]
+        L.emdb_host_unregister.argtypes = [VP]
         L.emdb_host_bytes.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
                                       ctypes.POINTER(ctypes.c_ulonglong)]
         L.emdb_run_ragged.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]

@@ -160,6 +160,13 @@ int emdb_run_noalloc(const emdb_config* cfg, const double* signals, const double
  * (EMDB_STATUS_* bits) into *status. */
 int emdb_status(emdb_plan* plan, int* status, void* stream);
 
+/* Page-lock an existing host range (e.g. a memory-mapped trace file) so the
+ * host pipeline's copies read it by DMA in place, and release it again.
+ * read_only != 0 for ranges the device only reads (file mappings opened
+ * read-only).  No reference counterpart: the trace-file ingest step. */
+int emdb_host_register(void* ptr, size_t bytes, int read_only);
+int emdb_host_unregister(void* ptr);
+
 /* ---- learned queue order (no reference counterpart: the reference launches
  * one CTA per signal in index order, kernels.py:1366-1371).  All on the
  * current CUDA device, asynchronous on `stream`. ---- */
