@@ -3,9 +3,12 @@
 N]`` plus the per-trace counts, batch by batch through the host pipeline
 (``emdb_run_host``).
 
-* Input is read in place: the file is memory-mapped read-only and each batch's
-  range is page-locked (``emdb_host_register``), so the host pipeline's copies
-  read the page cache by DMA -- no staging copy of the traces.
+* Input: the file is memory-mapped read-only.  Each batch's range is
+  page-locked in place (``emdb_host_register``) so the host pipeline's copies
+  read the page cache by DMA with no staging copy.  Where the operating system
+  refuses to pin file pages (recent Linux kernels refuse long-term pins of
+  file-backed memory), a reader thread copies batch k+1 into one of two
+  page-locked input buffers while the GPU works on batch k.
 * Output goes through two page-locked staging buffers: while the GPU works on
   batch k+1, a writer thread copies batch k's IMF rows into the output
   mapping (the OS writes them back to the file).
@@ -41,7 +44,8 @@ def decompose_file(in_path: str, out_path: str, batch: int = 16384, T=None,
     """Decompose every trace of ``in_path`` into ``out_path`` (a new .npy of
     IMF rows); returns ``{"n_imfs", "overflow", "debug_n", "debug_extno",
     "debug_nzm"}`` as NumPy arrays plus ``"batches_in_place"``, the number of
-    batches whose input pages were locked and read in place.  ``T`` as for
+    batches whose input pages were locked and read in place, and
+    ``"register_error"``, why they were not (None if they were).  ``T`` as for
     GPUBatchEMD (None = arange).  Raises like GPUBatchEMD; warns
     (UserWarning) if any trace overflowed."""
     import torch
@@ -65,6 +69,27 @@ def decompose_file(in_path: str, out_path: str, batch: int = 16384, T=None,
              for _ in range(2)]
     stream = torch.cuda.current_stream(launcher.device).cuda_stream
     x_ptr = X.ctypes.data if ntr else 0
+    bounds = [(s, min(ntr, s + batch)) for s in range(0, ntr, batch)]
+
+    # in place if the first batch's pages can be locked, else staged
+    reg_error = None
+    in_place_ok = False
+    if bounds:
+        lo, nb = _page_range(x_ptr, (bounds[0][1] - bounds[0][0]) * N * 8)
+        if L.emdb_host_register(ctypes.c_void_p(lo), nb, 1) == _native.EMDB_OK:
+            _native.check(L.emdb_host_unregister(ctypes.c_void_p(lo)), "emdb_host_unregister")
+            in_place_ok = True
+        else:
+            reg_error = _native.last_error()
+    stage_in = None if in_place_ok else [torch.empty((batch, N), dtype=torch.float64).pin_memory()
+                                         for _ in range(2)]
+
+    def load(k: int, s: int, e: int) -> None:
+        dst = stage_in[k].numpy()[: e - s]
+        parts = np.array_split(np.arange(e - s), max(1, min(writers, e - s)))
+        with cf.ThreadPoolExecutor(max_workers=len(parts)) as ex:
+            list(ex.map(lambda p: np.copyto(dst[p[0]: p[-1] + 1], X[s + p[0]: s + p[-1] + 1])
+                        if p.size else None, parts))
 
     def write_back(k: int, s: int, e: int) -> None:
         imfs, small = stage[k]
@@ -79,18 +104,24 @@ def decompose_file(in_path: str, out_path: str, batch: int = 16384, T=None,
 
     pending = [None, None]
     in_place = 0
-    with cf.ThreadPoolExecutor(max_workers=1) as writer:
-        for bi, s in enumerate(range(0, ntr, batch)):
-            e = min(ntr, s + batch)
+    with cf.ThreadPoolExecutor(max_workers=1) as writer, \
+            cf.ThreadPoolExecutor(max_workers=1) as reader:
+        loaded = None if in_place_ok or not bounds else reader.submit(load, 0, *bounds[0])
+        for bi, (s, e) in enumerate(bounds):
             k = bi % 2
             if pending[k] is not None:
-                pending[k].result()          # staging buffer k free again
-            ptr = x_ptr + s * N * 8
-            lo, nb = _page_range(ptr, (e - s) * N * 8)
-            # page-lock the batch's pages in place; if this system refuses to
-            # lock file pages the copies still work, staged by the driver
-            registered = L.emdb_host_register(ctypes.c_void_p(lo), nb, 1) == _native.EMDB_OK
-            in_place += int(registered)
+                pending[k].result()          # output staging buffer k free again
+            registered = False
+            if in_place_ok:
+                ptr = x_ptr + s * N * 8
+                lo, nb = _page_range(ptr, (e - s) * N * 8)
+                registered = L.emdb_host_register(ctypes.c_void_p(lo), nb, 1) == _native.EMDB_OK
+                in_place += int(registered)
+            else:
+                loaded.result()              # batch bi is in stage_in[k]
+                ptr = stage_in[k].data_ptr()
+                if bi + 1 < len(bounds):     # its buffer's last reader (batch bi-1) has returned
+                    loaded = reader.submit(load, (bi + 1) % 2, *bounds[bi + 1])
             try:
                 imfs, small = stage[k]
                 _native.check(L.emdb_run_host(
@@ -116,4 +147,5 @@ def decompose_file(in_path: str, out_path: str, batch: int = 16384, T=None,
             "output is not a verified decomposition. Check the `overflow` array to find which, "
             "and raise EMDKernelConfig.max_extrema / max_iteration for those.", stacklevel=2)
     res["batches_in_place"] = in_place
+    res["register_error"] = reg_error
     return res

@@ -30,7 +30,7 @@ def test_decompose_file_equals_device(tmp_path, with_T):
     assert np.array_equal(res["overflow"], o.cpu().numpy())
     for k, d in zip(("debug_n", "debug_extno", "debug_nzm"), emd.last_debug):
         assert np.array_equal(res[k], d.cpu().numpy())
-    print("batches read in place:", res["batches_in_place"], "of 3")
+    print("batches read in place:", res["batches_in_place"], "of 3;", res["register_error"])
 
 
 def test_decompose_file_rejects_bad_input(tmp_path):
