@@ -17,18 +17,27 @@
 //    kernels.py:722-726).  The post-update scan of pass n is reused as the
 //    pre-scan of pass n+1 (the reference scans the same data twice,
 //    kernels.py:930 vs 965);
-//  * boundary mirroring runs on one warp;
+//  * boundary mirroring runs on one warp (decisions on one lane);
 //  * the upper and lower not-a-knot systems are solved concurrently by
 //    parallel cyclic reduction (ping-pong buffers, one barrier per level);
 //  * envelope evaluation, the mean update and the six stop-test partial
 //    sums are one fused pass; sums are formed in the reference's order (128
 //    strided lanes + halving tree) and this file is compiled with
 //    -fmad=false, so every value equals the reference algorithm's FP64
-//    result bit for bit (the CPU oracle checks this).
+//    result bit for bit (the CPU oracle checks this);
+//  * every quotient is the IEEE one, but most are formed without the
+//    hardware division's slow-path branch: Markstein corrections from a
+//    reciprocal (RN(1/h) from a compile-time table on the integer time axis,
+//    where one correction is exact for integer operands), and for the PCR
+//    rows a branch-free division from the approximate reciprocal; each
+//    redoes its operation with the division outside the exact ranges.
 //
-// Per-pass knot/PCR storage is carved from the CTA's shared-memory arena; a
-// pass whose knots do not fit runs the same code on a per-CTA global slab.
-// Nothing here waits on another CTA.
+// Per-pass knot/PCR storage is placed by size: all in the CTA's shared-
+// memory arena; "borrow" (the proto-IMF parked in the per-CTA global slab
+// during the spline solve so both PCR buffers stay on-chip); "split" (PCR
+// buffer 1 in the slab); or all in the slab.  For the host pipeline the
+// kernel also reports finished chunks of traces through flags in mapped host
+// memory.  Nothing here waits on another CTA or on the host.
 
 #include "emdb_internal.cuh"
 
