@@ -77,3 +77,44 @@ def test_random_case_matches_oracle(k):
         np.testing.assert_array_equal(de[b], r.debug_extno, err_msg=str(ctx))
         np.testing.assert_array_equal(dz[b], r.debug_nzm, err_msg=str(ctx))
         assert _sha(imfs[b]) == _sha(r.imfs), ctx
+
+
+N_RAGGED = 24
+
+
+@pytest.mark.parametrize("k", range(N_RAGGED))
+def test_random_ragged_case_matches_oracle(k):
+    """CSR batches of mixed lengths in one launch, with a per-trace time axis
+    (each normalised on its own) or none, a random queue order and a random
+    configuration: every trace equals the oracle bit for bit."""
+    import torch
+    from cuda_emd import EMDKernelConfig, workloads as W
+    from oracle import emd_oracle as O
+    rng = np.random.default_rng(5000 + k)
+    cfg = dict(max_extrema=int(rng.choice([32, 256, 1024])), nbsym=int(rng.choice([1, 2, 3])),
+               max_iteration=int(rng.choice([10, 100])), max_imfs=int(rng.choice([4, 16])))
+    lens = rng.integers(3, 1500, size=int(rng.integers(3, 12)))
+    rows = [W.sinusoid_trace(rng, int(n)) if rng.random() < 0.5 else
+            np.cumsum(rng.standard_normal(int(n))) for n in lens]
+    per_T = rng.random() < 0.5
+    Ts = [O.normalise_T(np.cumsum(rng.uniform(0.5, 1.5, int(n))), int(n)) if per_T
+          else np.arange(int(n), dtype=np.float64) for n in lens]
+    offs = np.zeros(len(rows) + 1, dtype=np.int64)
+    np.cumsum(lens, out=offs[1:])
+    v = torch.from_numpy(np.concatenate(rows)).cuda()
+    o = torch.from_numpy(offs).cuda()
+    Td = torch.from_numpy(np.concatenate(Ts)).cuda() if per_T else None
+    order = torch.from_numpy(rng.permutation(len(rows)).astype(np.int32)).cuda()
+    L = EMDKernelConfig(threads_per_block=128, **cfg).build()
+    imfs, n_imfs, ovf, dn, de, dz = (x.cpu().numpy() for x in
+                                     L.run_ragged(v, o, order=order, T=Td, t_per_trace=True))
+    L.check_status()
+    mi = cfg["max_imfs"]
+    ocfg = O.OracleConfig(threads_per_block=128, **cfg)
+    for b, x in enumerate(rows):
+        r = O.emd_signal(x, Ts[b], ocfg)
+        ctx = (k, cfg, int(lens[b]), per_T, b)
+        assert n_imfs[b] == r.n_imfs and ovf[b] == r.overflow, ctx
+        np.testing.assert_array_equal(dn[b], r.debug_n, err_msg=str(ctx))
+        block = imfs[mi * offs[b]: mi * offs[b + 1]].reshape(mi, int(lens[b]))
+        assert _sha(block) == _sha(r.imfs), ctx
