@@ -1223,7 +1223,7 @@ __device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int 
   const int c = b / p.chunk_traces;
   atomicMax(p.chunk_rows + c, (unsigned)max(nim, 0));
   __threadfence();
-  const unsigned need = (unsigned)min(p.chunk_traces, p.batch - c * p.chunk_traces);
+  const unsigned need = (unsigned)min(p.chunk_traces, p.chunk_span - c * p.chunk_traces);
   if (atomicAdd(p.chunk_count + c, 1u) + 1u == need) {
     const unsigned rows = atomicMax(p.chunk_rows + c, 0u);
     __threadfence_system();

@@ -51,6 +51,17 @@ struct emdb_plan {
   std::mutex mu;
 };
 
+// Per-trace completion flags for ragged launches (emdb_run_ragged_notify):
+// device counters and row maxima, and flags in mapped host memory.
+struct emdb_notify {
+  int device = 0;
+  int capacity = 0;
+  unsigned* d_count = nullptr;
+  unsigned* d_rows = nullptr;
+  unsigned* h_flag = nullptr;   // pinned, mapped
+  unsigned* d_flag = nullptr;   // its device alias
+};
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -506,6 +517,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     sp.dbg_nzm = d_dz + t0 * mi;
     sp.queue = p->d_group_queue + k;
     sp.slab = p->d_group_slab + slab_off;
+    sp.chunk_span = (int)cnt;
     sp.chunk_count = p->d_chunk_count + gstart[k] / chunk;
     sp.chunk_rows = p->d_chunk_rows + gstart[k] / chunk;
     sp.chunk_flag = p->d_chunk_flag + gstart[k] / chunk;
@@ -586,15 +598,17 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   return EMDB_OK;
 }
 
-int emdb_run_ragged(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
-                    int max_n, const double* T, int t_per_trace, const int* order, double* imfs,
-                    int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
-                    void* stream) {
+static int run_ragged_impl(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
+                           int max_n, const double* T, int t_per_trace, const int* order,
+                           double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                           int* dbg_nzm, emdb_notify* nt, int n_traces, void* stream) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || max_n < 0) return fail(EMDB_ERR_INVALID, "batch and max_n must be >= 0");
   if (batch == 0) return EMDB_OK;
   if (!values || !offsets || !imfs || !n_imfs || !overflow || !dbg_n || !dbg_extno || !dbg_nzm)
     return fail(EMDB_ERR_INVALID, "NULL buffer");
+  if (nt && (n_traces < batch || n_traces > nt->capacity || nt->device != p->device))
+    return fail(EMDB_ERR_INVALID, "notify object too small or on another device");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   emdb::SiftParams sp{};
@@ -611,7 +625,80 @@ int emdb_run_ragged(emdb_plan* p, const double* values, const int64_t* offsets, 
   sp.dbg_n = dbg_n;
   sp.dbg_ext = dbg_extno;
   sp.dbg_nzm = dbg_nzm;
+  if (nt) {
+    sp.chunk_count = nt->d_count;
+    sp.chunk_rows = nt->d_rows;
+    sp.chunk_flag = nt->d_flag;
+    sp.chunk_traces = 1;
+    sp.chunk_span = n_traces;
+  }
   return launch_common(p, sp, max_n, (cudaStream_t)stream);
+}
+
+int emdb_run_ragged(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
+                    int max_n, const double* T, int t_per_trace, const int* order, double* imfs,
+                    int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
+                    void* stream) {
+  return run_ragged_impl(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs, n_imfs,
+                         overflow, dbg_n, dbg_extno, dbg_nzm, nullptr, 0, stream);
+}
+
+int emdb_run_ragged_notify(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
+                           int max_n, const double* T, int t_per_trace, const int* order,
+                           double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                           int* dbg_nzm, emdb_notify* notify, int n_traces, void* stream) {
+  if (!notify) return fail(EMDB_ERR_INVALID, "notify is NULL");
+  return run_ragged_impl(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs, n_imfs,
+                         overflow, dbg_n, dbg_extno, dbg_nzm, notify, n_traces, stream);
+}
+
+int emdb_notify_create(int capacity, int device, emdb_notify** out, unsigned** host_flags) {
+  if (!out || !host_flags || capacity < 1) return fail(EMDB_ERR_INVALID, "bad arguments");
+  *out = nullptr;
+  *host_flags = nullptr;
+  DeviceGuard g(device);
+  emdb_notify* nt = new emdb_notify();
+  nt->device = device;
+  nt->capacity = capacity;
+  cudaError_t e = cudaMalloc(&nt->d_count, capacity * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc(&nt->d_rows, capacity * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaHostAlloc(&nt->h_flag, capacity * sizeof(unsigned), cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer(&nt->d_flag, nt->h_flag, 0);
+  if (e == cudaSuccess) e = cudaMemset(nt->d_count, 0, capacity * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(nt->d_rows, 0, capacity * sizeof(unsigned));
+  if (e != cudaSuccess) {
+    emdb_notify_destroy(nt);
+    return cuda_fail(e, "allocating completion flags");
+  }
+  std::memset(nt->h_flag, 0, capacity * sizeof(unsigned));
+  *out = nt;
+  *host_flags = nt->h_flag;
+  return EMDB_OK;
+}
+
+int emdb_notify_reset(emdb_notify* nt, int n, void* stream) {
+  if (!nt || n < 0 || n > nt->capacity) return fail(EMDB_ERR_INVALID, "bad arguments");
+  DeviceGuard g(nt->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(nt->d_count, 0, n * sizeof(unsigned), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(nt->d_rows, 0, n * sizeof(unsigned), st);
+  if (e != cudaSuccess) return cuda_fail(e, "resetting completion counters");
+  // no launch that writes these flags is in flight (the caller's contract)
+  volatile unsigned* f = nt->h_flag;
+  for (int k = 0; k < n; ++k) f[k] = 0u;
+  return EMDB_OK;
+}
+
+int emdb_notify_destroy(emdb_notify* nt) {
+  if (!nt) return EMDB_OK;
+  {
+    DeviceGuard g(nt->device);
+    if (nt->d_count) cudaFree(nt->d_count);
+    if (nt->d_rows) cudaFree(nt->d_rows);
+    if (nt->h_flag) cudaFreeHost(nt->h_flag);
+  }
+  delete nt;
+  return EMDB_OK;
 }
 
 int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batch, int N,

@@ -49,6 +49,7 @@ struct SiftParams {
   unsigned* chunk_rows;       // device: the chunk's largest n_imfs, zeroed before launch
   unsigned* chunk_flag;       // mapped host flags: 1 + rows to copy once chunk c is complete
   int chunk_traces;
+  int chunk_span;             // traces the chunk indices cover (the last chunk may be short)
   // config (EMDKernelConfig fields)
   int max_extrema;
   int nbsym;

@@ -10,6 +10,8 @@ import ctypes
 import os
 import threading
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libemdb200.so")
 
@@ -29,7 +31,9 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
            "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena",
-           "emdb_host_bytes", "emdb_host_register", "emdb_host_unregister")
+           "emdb_host_bytes", "emdb_host_register", "emdb_host_unregister",
+           "emdb_notify_create", "emdb_notify_reset", "emdb_notify_destroy",
+           "emdb_run_ragged_notify")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -65,6 +69,11 @@ def load() -> ctypes.CDLL:
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_min_arena.argtypes = [I, ctypes.POINTER(I)]
+        L.emdb_notify_create.argtypes = [I, I, ctypes.POINTER(VP),
+                                         ctypes.POINTER(ctypes.POINTER(ctypes.c_uint))]
+        L.emdb_notify_reset.argtypes = [VP, I, VP]
+        L.emdb_notify_destroy.argtypes = [VP]
+        L.emdb_run_ragged_notify.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP, I, VP]
         L.emdb_host_register.argtypes = [VP, ctypes.c_size_t, I]
         L.emdb_host_unregister.argtypes = [VP]
         L.emdb_host_bytes.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
@@ -106,6 +115,34 @@ def check(rc: int, what: str) -> None:
     if rc == EMDB_ERR_NOMEM:
         raise MemoryError(msg)
     raise EmdbError(rc, msg)
+
+
+class Notify:
+    """Per-trace completion flags (emdb_notify): ``flags`` is a live NumPy view
+    of page-locked host memory the kernel writes; flags[b] = 1 + the rows of
+    trace b that may hold data, once trace b is complete (0 before)."""
+
+    def __init__(self, capacity: int, device: int):
+        self.L = load()
+        self.capacity = int(capacity)
+        h = ctypes.c_void_p()
+        ptr = ctypes.POINTER(ctypes.c_uint)()
+        check(self.L.emdb_notify_create(self.capacity, int(device), ctypes.byref(h),
+                                        ctypes.byref(ptr)), "emdb_notify_create")
+        self.handle = h
+        self.flags = np.ctypeslib.as_array(ptr, shape=(self.capacity,))
+
+    def reset(self, n: int, stream: int) -> None:
+        """Zero the first n counters and flags (no launch using them may run)."""
+        check(self.L.emdb_notify_reset(self.handle, int(n), stream), "emdb_notify_reset")
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.L.emdb_notify_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
 
 
 class Plan:

@@ -11,6 +11,12 @@ the CTAs of newly admitted ones: the work of old and new requests overlaps on
 the device.  Inside an admitted batch the queue order is longest-predicted-
 first when a cost model is attached (order never changes a result).
 
+Each trace of a launch raises a completion flag in page-locked host memory
+when its outputs are written (``emdb_run_ragged_notify``); as soon as all of
+a request's traces are flagged, that request's rows are copied back on a copy
+stream and the request is delivered -- it does not wait for the other
+requests of its launch.
+
 Per request the server records arrival, admission, device completion and
 host delivery times; ``latency = delivered - arrival``.
 """
@@ -50,10 +56,14 @@ class Request:
 class _Flight:
     slot: int
     reqs: list
-    event: object
-    outs: tuple
+    event: object                     # after every kernel of the launch
+    outs: tuple                       # host (imfs, n_imfs, overflow), page-locked
+    dev: tuple                        # device (imfs, n_imfs, overflow)
     offsets_h: np.ndarray
     budget: int
+    first: list                       # first trace index of each request
+    state: list                       # per request: 0 running, 1 copying, 2 delivered
+    copies: list                      # per request: event of its copy-back
     keep: tuple = field(default_factory=tuple)
 
 
@@ -69,7 +79,10 @@ class EMDServer:
         self.max_batch = max_batch_traces
         self.cost_model = cost_model
         self.streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
+        self.copy_stream = torch.cuda.Stream(self.device)
+        self.notify = [_native.Notify(max_batch_traces, self.device) for _ in range(slots)]
         self.plans: dict[tuple[int, int], _native.Plan] = {}
+        self.tier_streams: dict = {}
         self.free_slots = collections.deque(range(slots))
         self.pending: collections.deque[Request] = collections.deque()
         self.flights: list[_Flight] = []
@@ -90,6 +103,15 @@ class EMDServer:
     def _cost_bytes(n_samples: int, n_traces: int, max_imfs: int) -> int:
         # input + dense CSR output + per-trace counts (and the offsets / order)
         return n_samples * 8 * (1 + max_imfs) + n_traces * (4 * 3 * max_imfs + 24)
+
+    def _tier_stream(self, slot: int, edge: int):
+        import torch
+        key = (slot, edge)
+        t = self.tier_streams.get(key)
+        if t is None:
+            t = torch.cuda.Stream(self.device)
+            self.tier_streams[key] = t
+        return t
 
     def _plan(self, slot: int, edge: int) -> _native.Plan:
         key = (slot, edge)
@@ -137,6 +159,8 @@ class EMDServer:
             r.admitted = now
         mi = self.cfg.max_imfs
         dev = torch.device("cuda", self.device)
+        nt = self.notify[slot]
+        nt.reset(ntr, st.cuda_stream)          # the slot's previous launch has finished
         with torch.cuda.stream(st):
             vals = torch.from_numpy(vals_h).pin_memory().to(dev, non_blocking=True)
             offs = torch.from_numpy(off_h).pin_memory().to(dev, non_blocking=True)
@@ -153,6 +177,7 @@ class EMDServer:
                 cost = predicted_cost(self.cost_model, f, offs[1:] - offs[:-1])
             edges = np.array([tier_of(int(n)) for n in lens])
             keep = [vals, offs]
+            tiers = []
             for e in sorted(set(edges.tolist()), reverse=True):
                 idx = np.flatnonzero(edges == e)
                 order = torch.from_numpy(idx.astype(np.int32)).to(dev, non_blocking=True)
@@ -160,51 +185,98 @@ class EMDServer:
                     sub = cost[order.long()]
                     order = order[torch.argsort(sub, descending=True, stable=True)]
                 keep.append(order)
-                p = self._plan(slot, e)
-                _native.check(p.L.emdb_run_ragged(
-                    p.handle, vals.data_ptr(), offs.data_ptr(), int(idx.size), int(e), None, 1,
-                    order.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
-                    dn.data_ptr(), de.data_ptr(), dz.data_ptr(), st.cuda_stream), "emdb_run_ragged")
-            h_imfs = torch.empty(mi * nsamp, dtype=torch.float64).pin_memory()
-            h_n = torch.empty(ntr, dtype=torch.int32).pin_memory()
-            h_o = torch.empty(ntr, dtype=torch.int32).pin_memory()
-            h_imfs.copy_(imfs, non_blocking=True)
-            h_n.copy_(n_imfs, non_blocking=True)
-            h_o.copy_(ovf, non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(st)
-        keep.extend([imfs, n_imfs, ovf, dn, de, dz])
-        self.flights.append(_Flight(slot, reqs, ev, (h_imfs, h_n, h_o), off_h, budget, tuple(keep)))
+                tiers.append((e, idx.size, order))
+            ready = torch.cuda.Event()
+            ready.record(st)
+        # each tier on its own stream of the slot, so a short tier's traces
+        # (and the requests they finish) need not wait for a long tier
+        for e, cnt, order in tiers:
+            ts = self._tier_stream(slot, e)
+            ts.wait_event(ready)
+            p = self._plan(slot, e)
+            _native.check(p.L.emdb_run_ragged_notify(
+                p.handle, vals.data_ptr(), offs.data_ptr(), int(cnt), int(e), None, 1,
+                order.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
+                dn.data_ptr(), de.data_ptr(), dz.data_ptr(), nt.handle, ntr, ts.cuda_stream),
+                "emdb_run_ragged_notify")
+            done_t = torch.cuda.Event()
+            done_t.record(ts)
+            st.wait_event(done_t)
+        ev = torch.cuda.Event()
+        ev.record(st)
+        h_imfs = torch.empty(mi * nsamp, dtype=torch.float64).pin_memory()
+        h_n = torch.empty(ntr, dtype=torch.int32).pin_memory()
+        h_o = torch.empty(ntr, dtype=torch.int32).pin_memory()
+        first, k = [], 0
+        for r in reqs:
+            first.append(k)
+            k += len(r.traces)
+        first.append(k)
+        keep.extend([dn, de, dz])
+        self.flights.append(_Flight(slot, reqs, ev, (h_imfs, h_n, h_o), (imfs, n_imfs, ovf), off_h,
+                                    budget, first, [0] * len(reqs), [None] * len(reqs), tuple(keep)))
 
     # -- completion -------------------------------------------------------------
+    def _copy_request(self, f: _Flight, q: int, flags: np.ndarray) -> None:
+        """Copy request q's rows (only those that may hold data) and counts back."""
+        import torch
+        h_imfs, h_n, h_o = f.outs
+        d_imfs, d_n, d_o = f.dev
+        mi = self.cfg.max_imfs
+        k0, k1 = f.first[q], f.first[q + 1]
+        with torch.cuda.stream(self.copy_stream):
+            for k in range(k0, k1):
+                a, b = int(f.offsets_h[k]), int(f.offsets_h[k + 1])
+                # a flag still 0 here means the launch ended without it: copy all rows
+                rows = mi if int(flags[k]) == 0 else min(int(flags[k]) - 1, mi)
+                if rows > 0:
+                    h_imfs[mi * a: mi * a + rows * (b - a)].copy_(
+                        d_imfs[mi * a: mi * a + rows * (b - a)], non_blocking=True)
+            h_n[k0:k1].copy_(d_n[k0:k1], non_blocking=True)
+            h_o[k0:k1].copy_(d_o[k0:k1], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(self.copy_stream)
+        f.copies[q] = ev
+        f.state[q] = 1
+
+    def _deliver(self, f: _Flight, q: int) -> None:
+        h_imfs, h_n, h_o = (x.numpy() for x in f.outs)
+        mi = self.cfg.max_imfs
+        r = f.reqs[q]
+        rows, nims, ovfs = [], [], []
+        for k in range(f.first[q], f.first[q + 1]):
+            a, b = int(f.offsets_h[k]), int(f.offsets_h[k + 1])
+            blk = h_imfs[mi * a: mi * b].reshape(mi, b - a)
+            rows.append(blk[:int(h_n[k])].copy())
+            nims.append(int(h_n[k]))
+            ovfs.append(int(h_o[k]))
+        r.done = self.now()
+        r.result = (rows, np.array(nims, dtype=np.int32), np.array(ovfs, dtype=np.int32))
+        r.delivered = self.now()
+        self.completed.append(r)
+        f.state[q] = 2
+
     def _reap(self) -> int:
+        """Deliver every request whose traces are all done; release a slot once
+        its launch has finished and all its requests are delivered."""
         done = 0
         still = []
         for f in self.flights:
-            if not f.event.query():
+            flags = self.notify[f.slot].flags
+            kernels_done = f.event.query()
+            for q in range(len(f.reqs)):
+                if f.state[q] == 0:
+                    k0, k1 = f.first[q], f.first[q + 1]
+                    if kernels_done or (flags[k0:k1] != 0).all():
+                        self._copy_request(f, q, flags)
+                if f.state[q] == 1 and f.copies[q].query():
+                    self._deliver(f, q)
+                    done += 1
+            if kernels_done and all(st == 2 for st in f.state):
+                self.in_use -= f.budget
+                self.free_slots.append(f.slot)
+            else:
                 still.append(f)
-                continue
-            t = self.now()
-            h_imfs, h_n, h_o = (x.numpy() for x in f.outs)
-            mi = self.cfg.max_imfs
-            k = 0
-            for r in f.reqs:
-                rows, nims, ovfs = [], [], []
-                for tr in r.traces:
-                    N = tr.shape[0]
-                    a, b = f.offsets_h[k], f.offsets_h[k + 1]
-                    blk = h_imfs[mi * a: mi * b].reshape(mi, N)
-                    rows.append(blk[:int(h_n[k])].copy())
-                    nims.append(int(h_n[k]))
-                    ovfs.append(int(h_o[k]))
-                    k += 1
-                r.done = t
-                r.result = (rows, np.array(nims, dtype=np.int32), np.array(ovfs, dtype=np.int32))
-                r.delivered = self.now()
-                self.completed.append(r)
-            self.in_use -= f.budget
-            self.free_slots.append(f.slot)
-            done += len(f.reqs)
         self.flights = still
         return done
 

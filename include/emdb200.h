@@ -122,6 +122,27 @@ int emdb_run_ragged(emdb_plan* plan, const double* values, const int64_t* offset
                     double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                     int* dbg_nzm, void* stream);
 
+/* Per-trace completion flags for ragged launches, so a caller can take each
+ * trace's results as soon as that trace is done instead of at the end of the
+ * launch (the serving loop delivers each request this way).  No reference
+ * counterpart.  create: capacity traces; *host_flags is page-locked host
+ * memory the kernel writes: host_flags[b] becomes 1 + the number of rows of
+ * trace b that may hold data once all of trace b's outputs are written.
+ * reset: zero the first n counters (asynchronously on `stream`) and host
+ * flags (immediately) -- only while no launch that uses the object runs. */
+typedef struct emdb_notify emdb_notify;
+int emdb_notify_create(int capacity, int device, emdb_notify** out, unsigned** host_flags);
+int emdb_notify_reset(emdb_notify* notify, int n, void* stream);
+int emdb_notify_destroy(emdb_notify* notify);
+/* emdb_run_ragged that also raises trace b's completion flag (b is the
+ * trace's index in offsets; n_traces = the number of traces offsets holds,
+ * <= the notify object's capacity). */
+int emdb_run_ragged_notify(emdb_plan* plan, const double* values, const int64_t* offsets,
+                           int batch, int max_n, const double* T, int t_per_trace,
+                           const int* order, double* imfs, int* n_imfs, int* overflow,
+                           int* dbg_n, int* dbg_extno, int* dbg_nzm, emdb_notify* notify,
+                           int n_traces, void* stream);
+
 /* Extrema + mirroring + both envelopes on raw traces, no sift loop
  * (run_envelope_only): max_env/min_env [batch, N], n_extrema [batch, 2],
  * degenerate [batch], knot positions/values [batch, mbuf] each with

@@ -83,3 +83,32 @@ def test_server_hbm_budget_limits_admission():
     assert len(srv.flights) == 1          # the budget admits one request at a time
     srv.drain(timeout_s=120)
     assert all(r.result is not None for r in reqs)
+
+
+def test_short_request_is_not_held_by_a_long_one():
+    """Two requests admitted into one launch: one long chirp (thousands of
+    extrema, a long sift) and one short trace.  Each trace raises its own
+    completion flag, the tiers run side by side, and the short request is
+    delivered as soon as its trace is done -- long before the launch ends --
+    with the same results as when served alone."""
+    from cuda_emd import workloads as W
+    from cuda_emd.serving import EMDServer, Request
+    rng = np.random.default_rng(8)
+    long_tr, short_tr = W.chirp_trace(rng, 8192), W.sinusoid_trace(rng, 256)
+    alone = EMDServer(slots=1)
+    solo = Request(9, [short_tr])
+    alone.submit(solo)
+    alone.drain(timeout_s=120)
+    srv = EMDServer(slots=1)
+    a, b = Request(0, [long_tr]), Request(1, [short_tr])
+    srv.submit(a)
+    srv.submit(b)
+    srv.drain(timeout_s=120)
+    srv.check_status()
+    assert a.admitted == b.admitted                 # one launch for both
+    la, lb = a.delivered - a.admitted, b.delivered - b.admitted
+    print(f"long request {la * 1e3:.1f} ms, short request {lb * 1e3:.1f} ms")
+    assert lb < 0.5 * la, (la, lb)
+    for x, y in zip(solo.result[0], b.result[0]):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(solo.result[1], b.result[1])
