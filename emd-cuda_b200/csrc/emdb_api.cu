@@ -89,28 +89,33 @@ struct DeviceGuard {
   }
 };
 
-// Per-SM shared memory is 228 KB on B200 with 1 KB reserved per CTA; pick the
-// largest arena that still keeps `want` CTAs resident, but never below what a
-// trace of length max_n needs plus a modest knot budget.
+// Per-SM shared memory is 228 KB on B200 with 1 KB reserved per CTA.  The
+// arena for `want` resident CTAs is the largest share that keeps them all.
+// Choice: the most CTAs (up to the plan's register variant) whose arena holds
+// the trace plus room for ~2 x 96 knots; failing that, still 3 CTAs/SM if
+// that arena holds the trace at all, before fewer.  Measured on B200 with
+// seismic traces: N = 4096 ran 87 ms at 3 CTAs/SM (knot room) vs 108 ms at 4
+// (none); N = 8192 ran 688 ms at 3 CTAs/SM (knots spilled) vs 867 ms at 2:
+// below 12 warps per SM latency hiding collapses.
 int auto_arena(const emdb_plan* p, int max_n) {
   const int per_sm = 233472;
-  size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
-  int best = 0;
-  for (int want = p->variant; want >= 1; --want) {
-    int arena = per_sm / want - 1024;
-    arena = std::min(arena, p->smem_optin);
+  const size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
+  auto share = [&](int want) {
+    int arena = std::min(per_sm / want - 1024, p->smem_optin);
     // shared memory is allocated in 128-byte units: a 16-byte-rounded share
     // can round up past the SM's capacity and lose a CTA (e.g. 5 per SM)
-    arena &= ~127;
-    // need the fixed part plus room for ~2 x 96 knots before spilling
-    size_t min_need = fixed + (size_t)(11 * 2 * (96 + 2 * p->cfg.nbsym + 2)) * sizeof(double);
-    if ((size_t)arena >= min_need) { best = arena; break; }
-  }
-  if (best == 0) {
-    size_t need = fixed + 64;
-    if (need <= (size_t)p->smem_optin) best = (int)((need + 15) & ~size_t(15));
-  }
-  return best;
+    return arena & ~127;
+  };
+  const size_t knot_room = (size_t)(11 * 2 * (96 + 2 * p->cfg.nbsym + 2)) * sizeof(double);
+  for (int want = p->variant; want >= 1; --want)
+    if ((size_t)share(want) >= fixed + knot_room) {
+      if (want >= 3) return share(want);
+      break;                                   // would drop below 3 CTAs/SM
+    }
+  for (int want = std::min(p->variant, 3); want >= 1; --want)
+    if ((size_t)share(want) >= fixed + 64) return share(want);
+  const size_t need = fixed + 64;
+  return need <= (size_t)p->smem_optin ? (int)((need + 15) & ~size_t(15)) : 0;
 }
 
 int arena_for(const emdb_plan* p, int max_n) {
