@@ -50,6 +50,8 @@ WORKLOADS = {
     "seismic16k": dict(n=16384, N=2048, desc="16384 seismic traces x 2048 samples, dt 2 ms"),
     "sinusoid256": dict(n=256, N=1024, desc="256 three-tone traces x 1024 samples"),
     "seismic1k": dict(n=1024, N=2048, desc="1024 seismic traces x 2048 samples (profiling size)"),
+    "seismic8k": dict(n=2048, N=8192, desc="2048 seismic traces x 8192 samples (every trace overflows "
+                                           "max_extrema; knots in the per-CTA slab)"),
     "serve": dict(lo=512, hi=16384, max_traces=64,
                   desc="Poisson requests of 1-64 traces, N log-uniform [512, 16384], ragged mix; "
                        "offered load 10-110% of measured saturation"),
