@@ -44,6 +44,9 @@
 // Tuning knobs (compile-time; results are identical for every setting):
 //  EMDB_EVAL_PAIR  evaluate two samples per loop trip in the fused pass
 //  EMDB_PCR_PAIR   update two PCR rows per loop trip
+//  EMDB_OUTLINE    rarely taken paths as calls instead of inline copies:
+//                  1 the general evaluation and the binary segment search,
+//                  2 also the IEEE-division fallbacks of the PCR and setup rows
 //  EMDB_MERGED_PLACE  0: one sift-pass instance per knot placement; 1: one
 //                  for the on-chip placements and one for the off-chip ones
 //                  (placement chosen at run time); 2: one for all
@@ -82,6 +85,9 @@
 #endif
 #ifndef EMDB_PCR_PAIR
 #define EMDB_PCR_PAIR 0
+#endif
+#ifndef EMDB_OUTLINE
+#define EMDB_OUTLINE 2
 #endif
 #ifndef EMDB_FAST_DIV
 #define EMDB_FAST_DIV 3
@@ -317,6 +323,26 @@ enum : int { kOnChip = -1, kOffChip = -2, kAnyPlace = -3 };
 // outside that range, so a caller can redo a whole sample with the division
 // once instead of branching on every quotient.
 __device__ __noinline__ double div_slow(double a, double b) { return a / b; }
+
+// Rarely taken paths of the hot loops (fewer than 4 knots, operands outside
+// the fast quotients' range, knot lists that are not strictly increasing) as
+// calls to one out-of-line body each, instead of an inline copy per call site:
+// keeps the hot loops' code small.  Defined after eval_seg / search_seg.
+__device__ __noinline__ double eval_seg_cold(const double* x, const double* y, const double* M,
+                                             int n, double t, int lo);
+__device__ __noinline__ int search_seg_cold(const double* x, int n, double t);
+#if EMDB_OUTLINE >= 1
+#define EMDB_EVAL_RARE(sv, t, lo) eval_seg_cold((sv).x, (sv).y, (sv).M, (sv).n, (t), (lo))
+#define EMDB_SEARCH_RARE(sv, t) search_seg_cold((sv).x, (sv).n, (t))
+#else
+#define EMDB_EVAL_RARE(sv, t, lo) eval_seg((sv), (t), (lo))
+#define EMDB_SEARCH_RARE(sv, t) search_seg((sv), (t))
+#endif
+#if EMDB_OUTLINE >= 2
+#define EMDB_DIV_RARE(a, b) div_slow((a), (b))
+#else
+#define EMDB_DIV_RARE(a, b) ((a) / (b))
+#endif
 
 __device__ __forceinline__ double div_q(double a, double b, double y, bool& slow) {
   const double q0 = a * y;
@@ -756,7 +782,8 @@ __device__ __forceinline__ void setup_row(const double* x, const double* y, int 
       bool slow = !ok || (double)ji != h_i || (double)jm != h_im1;
       const double sr = div_q(y[i + 1] - y[i], h_i, g_rcp.v[ji], slow);
       const double sl = div_q(y[i] - y[i - 1], h_im1, g_rcp.v[jm], slow);
-      d = slow ? 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1) : 6.0 * (sr - sl);
+      d = slow ? 6.0 * (EMDB_DIV_RARE(y[i + 1] - y[i], h_i) - EMDB_DIV_RARE(y[i] - y[i - 1], h_im1))
+               : 6.0 * (sr - sl);
     } else {
       d = 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1);
     }
@@ -778,8 +805,8 @@ __device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* _
   double alpha = hl ? ql : 0.0;
   double beta = hr ? qr : 0.0;
   if ((hl && sl) || (hr && sr)) {
-    alpha = hl ? ak / b_left : 0.0;
-    beta = hr ? ck / b_right : 0.0;
+    alpha = hl ? EMDB_DIV_RARE(ak, b_left) : 0.0;
+    beta = hr ? EMDB_DIV_RARE(ck, b_right) : 0.0;
   }
 #else
   const double alpha = hl ? ak / b_left : 0.0;
@@ -915,7 +942,7 @@ __device__ __forceinline__ double eval_seg(const SideView& s, double t, int lo) 
 // the same operation order; sets `slow` when a quotient needs the division,
 // and the caller then re-evaluates the sample with eval_seg.
 __device__ __forceinline__ double eval_seg_q(const SideView& s, double t, int lo, bool& slow) {
-  if (s.n < 4) return eval_seg(s, t, lo);
+  if (s.n < 4) return EMDB_EVAL_RARE(s, t, lo);
   const double* x = s.x;
   const double* y = s.y;
   double x0 = x[lo], x1 = x[lo + 1];
@@ -946,6 +973,19 @@ __device__ __forceinline__ int search_seg(const SideView& s, double t) {
     if (s.x[mid] <= t) lo = mid; else hi = mid - 1;
   }
   return lo;
+}
+
+// Out-of-line bodies of the rare paths declared with div_slow.
+__device__ __noinline__ double eval_seg_cold(const double* x, const double* y, const double* M,
+                                             int n, double t, int lo) {
+  SideView s;
+  s.x = x; s.y = y; s.M = M; s.R = nullptr; s.n = n; s.nl = 0; s.nt = 0;
+  return eval_seg(s, t, lo);
+}
+__device__ __noinline__ int search_seg_cold(const double* x, int n, double t) {
+  SideView s;
+  s.x = x; s.y = nullptr; s.M = nullptr; s.R = nullptr; s.n = n; s.nl = 0; s.nt = 0;
+  return search_seg(s, t);
 }
 
 // 128-lane tree of the reference (kernels.py:794-804), on warp 0, for a value
@@ -998,7 +1038,7 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
 // sample with eval_seg.  Same operation order as eval_seg otherwise.
 __device__ __forceinline__ double eval_seg_int(const SideView& s, double t, int lo, bool& slow,
                                                bool sorted = false) {
-  if (s.n < 4) return eval_seg(s, t, lo);
+  if (s.n < 4) return EMDB_EVAL_RARE(s, t, lo);
   const double* x = s.x;
   const double* y = s.y;
   double x0 = x[lo], x1 = x[lo + 1];
@@ -1106,8 +1146,8 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       lo0 = min(max(k0 - 1, 0), sv0.n - 2);
       lo1 = min(max(k1 - 1, 0), sv1.n - 2);
     } else {
-      if (sv0.n >= 4) lo0 = search_seg(sv0, t);
-      if (sv1.n >= 4) lo1 = search_seg(sv1, t);
+      if (sv0.n >= 4) lo0 = EMDB_SEARCH_RARE(sv0, t);
+      if (sv1.n >= 4) lo1 = EMDB_SEARCH_RARE(sv1, t);
     }
   };
   // T is strictly increasing, so the knot spans cover every sample iff they
@@ -1145,10 +1185,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       }
     }
     if (slow) {
-      emax = eval_seg(sv0, t, lo0);
-      emin = eval_seg(sv1, t, lo1);
-      emax2 = eval_seg(sv0, t2, lo0b);
-      emin2 = eval_seg(sv1, t2, lo1b);
+      emax = EMDB_EVAL_RARE(sv0, t, lo0);
+      emin = EMDB_EVAL_RARE(sv1, t, lo1);
+      emax2 = EMDB_EVAL_RARE(sv0, t2, lo0b);
+      emin2 = EMDB_EVAL_RARE(sv1, t2, lo1b);
     }
 #else
     const double emax = eval_seg(sv0, t, lo0);
