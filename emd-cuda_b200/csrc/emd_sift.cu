@@ -35,9 +35,11 @@
 // Per-pass knot/PCR storage is placed by size: all in the CTA's shared-
 // memory arena; "borrow" (the proto-IMF parked in the per-CTA global slab
 // during the spline solve so both PCR buffers stay on-chip); "split" (PCR
-// buffer 1 in the slab); or all in the slab.  For the host pipeline the
-// kernel also reports finished chunks of traces through flags in mapped host
-// memory.  Nothing here waits on another CTA or on the host.
+// buffer 1 in the slab); "park" (the proto-IMF parked, PCR buffer 1 in its
+// place, the knots and buffer 0 in the slab); or all in the slab.  For the
+// host pipeline the kernel also reports finished chunks of traces through
+// flags in mapped host memory.  Nothing here waits on another CTA or on the
+// host.
 
 #include "emdb_internal.cuh"
 
@@ -304,7 +306,42 @@ __device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, in
   return K;
 }
 
-enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3 };
+// Park placement, for passes whose knots fit neither shared-memory placement
+// but whose PCR buffer 1 fits the proto-IMF's space (long traces with many
+// knots): the proto-IMF is parked in the slab as for the borrow placement,
+// buffer 1 takes its place (imf region plus the arena ahead), and X | Y |
+// buffer 0 go to the slab after the parked samples.  Half of the PCR levels
+// then read shared memory; the evaluation reads the knots and the old samples
+// from the slab.  The reduction lanes use the arena start, free after the
+// solve.
+__host__ __device__ inline bool park_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
+                                          int kc1) {
+  const size_t cap = (size_t)(kc0 + kc1);
+  const size_t imfb = align16((size_t)N * sizeof(double));
+  return EMDB_FAST_DIV != 1 && 4 * cap * sizeof(double) <= imfb + (size_t)arena_bytes &&
+         imfb + 6 * cap * sizeof(double) <= slab_stride;
+}
+
+__device__ __forceinline__ Knots place_knots_park(double* imf, char* slab, int N, int kc0, int kc1,
+                                                  double* red) {
+  Knots K;
+  K.cap = kc0 + kc1;
+  double* p = reinterpret_cast<double*>(slab + align16((size_t)N * sizeof(double)));
+  K.X[0] = p; p += kc0;
+  K.Y[0] = p; p += kc0;
+  K.X[1] = p; p += kc1;
+  K.Y[1] = p; p += kc1;
+  K.P[0] = p;
+  K.P[1] = imf;
+  K.M[0] = K.P[0];
+  K.M[1] = K.P[0] + 2 * K.cap;
+  K.R[0] = K.P[1];
+  K.R[1] = K.P[1] + 2 * K.cap;
+  K.red = red;
+  return K;
+}
+
+enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3, kPlacePark = 4 };
 enum : int { kOnChip = -1, kOffChip = -2, kAnyPlace = -3 };
 
 // Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
@@ -1077,10 +1114,11 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
                                               int lane, int place = kPlaceSmem) {
   // kGroup >= 0: one placement, fixed at compile time.  kGroup == kOnChip /
   // kOffChip: one instance for the on-chip (shared, borrow) or off-chip
-  // (split, slab) placements, chosen by `place` at run time.
+  // (split, park, slab) placements, chosen by `place` at run time.
   const int kPlace = kGroup >= 0 ? kGroup
                    : kGroup == kOnChip ? (place == kPlaceBorrow ? kPlaceBorrow : kPlaceSmem)
-                   : kGroup == kOffChip ? (place == kPlaceSplit ? kPlaceSplit : kPlaceSlab)
+                   : kGroup == kOffChip ? (place == kPlaceSplit ? kPlaceSplit
+                                           : place == kPlacePark ? kPlacePark : kPlaceSlab)
                                         : place;
   Ctl& C = *L.ctl;
   double* imf = L.imf;
@@ -1088,6 +1126,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   Knots K = kPlace == kPlaceSmem    ? place_knots(L.arena, kc0, kc1)
            : kPlace == kPlaceSplit  ? place_knots_split(L.arena, L.arena_bytes, slab, kc0, kc1)
            : kPlace == kPlaceBorrow ? place_knots_borrow(imf, L.arena, L.arena_bytes, slab, N, kc0, kc1)
+           : kPlace == kPlacePark   ? place_knots_park(imf, slab, N, kc0, kc1, L.red)
                                     : place_knots(slab, kc0, kc1);
   PassSums ps;
   bool bad = fill_true_knots(L, K, e, N, NB, T, warp, lane);
@@ -1095,7 +1134,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   bool mbad = false;
   if (warp == 0) {
     mbad = mirror_both(L, K, e, N, NB, T, lane);
-  } else if (kPlace == kPlaceBorrow) {
+  } else if (kPlace == kPlaceBorrow || kPlace == kPlacePark) {
     // park the proto-IMF while warp 0 mirrors; PCR buffer 1 overwrites it
     double* save = borrow_save(slab);
     for (int i = tid - 32; i < N; i += kThreads - 32) save[i] = imf[i];
@@ -1103,7 +1142,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   ps.bad = __syncthreads_or(bad || mbad) != 0;
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
   solve_splines<kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid);
-  const double* oldv = kPlace == kPlaceBorrow ? borrow_save(slab) : imf;
+  const double* oldv = (kPlace == kPlaceBorrow || kPlace == kPlacePark) ? borrow_save(slab) : imf;
 
   SideView sv0, sv1;
   sv0.x = K.X[0] + kb0; sv0.y = K.Y[0] + kb0; sv0.M = K.M[0]; sv0.R = K.R[0];
@@ -1351,6 +1390,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
           const int place = knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSmem
                           : borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlaceBorrow
                           : split_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSplit
+                          : park_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlacePark
                                                                          : kPlaceSlab;
           if (EMDB_MERGED_PLACE == 2)
             flags = sift_pass<kAnyPlace, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
@@ -1368,6 +1408,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
           ++spilled;
         } else if (split_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
           flags = sift_pass<kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          ++spilled;
+        } else if (park_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
+          flags = sift_pass<kPlacePark, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         } else {
           flags = sift_pass<kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane);

@@ -252,6 +252,25 @@ def test_arena_sizes_same_results(arena):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("N,arena", [(8192, 76800), (4096, 57344)])
+def test_park_placement_same_results(N, arena):
+    """Long traces with many knots (seismic noise past max_extrema, a chirp):
+    at 3-4 CTAs/SM their passes park the proto-IMF in the slab and put PCR
+    buffer 1 in its place; at one CTA/SM the knots stay on-chip.  Same bits."""
+    import torch
+    from cuda_emd import EMDKernelConfig, workloads as W
+    rng = np.random.default_rng(311)
+    X = np.concatenate([W.seismic_batch(5, N, seed=310), W.chirp_trace(rng, N)[None, :]])
+    L = EMDKernelConfig().build()
+    L._plan.set_arena(232448)
+    ref = [o.cpu() for o in L.run(torch.from_numpy(X).cuda(), None)]
+    L._plan.set_arena(arena)
+    out = [o.cpu() for o in L.run(torch.from_numpy(X).cuda(), None)]
+    L.check_status()
+    for a, b in zip(ref, out):
+        assert torch.equal(a, b)
+
+
 def test_arena_too_small_raises():
     import torch
     from cuda_emd import EMDKernelConfig
