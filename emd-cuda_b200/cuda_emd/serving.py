@@ -17,6 +17,12 @@ a request's traces are flagged, that request's rows are copied back on a copy
 stream and the request is delivered -- it does not wait for the other
 requests of its launch.
 
+Each tier launch takes the largest shared-memory arena that still lets every
+trace in flight be resident: on a lightly loaded GPU a long trace gets an SM
+to itself with its knots on-chip (a sift that is latency-bound runs fastest
+there), and once the traces in flight need 3 or more CTAs per SM the plan's
+own throughput rule applies.  The arena never changes a result.
+
 Per request the server records arrival, admission, device completion and
 host delivery times; ``latency = delivered - arrival``.
 """
@@ -70,10 +76,16 @@ class _Flight:
 class EMDServer:
     def __init__(self, config: EMDKernelConfig | None = None, device: int | None = None,
                  slots: int = 4, hbm_budget_bytes: int = 32 << 30, max_batch_traces: int = 4096,
-                 cost_model=None):
+                 cost_model=None, adaptive_arena: bool = True):
         import torch
         self.cfg = config or EMDKernelConfig()
         self.device = torch.cuda.current_device() if device is None else int(device)
+        props = torch.cuda.get_device_properties(self.device)
+        self.num_sms = props.multi_processor_count
+        self.smem_sm = props.shared_memory_per_multiprocessor
+        self.smem_optin = props.shared_memory_per_block_optin
+        self.adaptive_arena = adaptive_arena
+        self.min_arena: dict[int, int] = {}
         self.nslots = slots
         self.budget = int(hbm_budget_bytes)
         self.max_batch = max_batch_traces
@@ -120,6 +132,23 @@ class EMDServer:
             p = _native.Plan(self.cfg.to_c(), self.device)
             self.plans[key] = p
         return p
+
+    def _tier_arena(self, edge: int, in_flight: int) -> int:
+        """Arena for a tier launch of traces up to `edge` samples while
+        `in_flight` traces (this launch's included) are on the GPU: the largest
+        one that still lets them all be resident when that takes 1 or 2 CTAs
+        per SM, else 0 (the plan's rule)."""
+        if not self.adaptive_arena:
+            return 0
+        per_sm = max(1, -(-in_flight // self.num_sms))
+        if per_sm > 2:
+            return 0
+        # the driver reserves 1 KB per CTA; allocation is in 128-byte units
+        arena = min(self.smem_sm // per_sm - 1024, self.smem_optin) & ~127
+        m = self.min_arena.get(edge)
+        if m is None:
+            m = self.min_arena[edge] = self._plan(0, edge).min_arena(edge)
+        return arena if arena >= m else 0
 
     def _admit(self) -> int:
         """Admit pending requests into free slots while the budget allows."""
@@ -190,10 +219,12 @@ class EMDServer:
             ready.record(st)
         # each tier on its own stream of the slot, so a short tier's traces
         # (and the requests they finish) need not wait for a long tier
+        in_flight = ntr + sum(f.first[-1] for f in self.flights)
         for e, cnt, order in tiers:
             ts = self._tier_stream(slot, e)
             ts.wait_event(ready)
             p = self._plan(slot, e)
+            p.set_arena(self._tier_arena(e, in_flight))
             _native.check(p.L.emdb_run_ragged_notify(
                 p.handle, vals.data_ptr(), offs.data_ptr(), int(cnt), int(e), None, 1,
                 order.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
