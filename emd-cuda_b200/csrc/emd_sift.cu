@@ -34,7 +34,8 @@
 //
 // Per-pass knot/PCR storage is placed by size: all in the CTA's shared-
 // memory arena; "borrow" (the proto-IMF parked in the per-CTA global slab
-// during the spline solve so both PCR buffers stay on-chip); "split" (PCR
+// during the spline solve so both PCR buffers stay on-chip, or with the
+// moments beside the knots when the arena is short); "split" (PCR
 // buffer 1 in the slab); "park" (the proto-IMF parked, PCR buffer 1 in its
 // place, the knots and buffer 0 in the slab); or all in the slab.  For the
 // host pipeline the kernel also reports finished chunks of traces through
@@ -306,6 +307,41 @@ __device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, in
   return K;
 }
 
+// Compact borrow placement, for long traces whose X | Y | buffer 0 do not fit
+// the arena next to the proto-IMF: the moments get their own array beside the
+// knots (instead of buffer 0's dead a / c arrays), so only X | Y | M sit at the
+// arena's end and both PCR buffers go to the front of the proto-IMF region
+// (parked in the slab, as for the borrow placement).  Everything stays
+// on-chip; the arena needs 3 doubles per knot slot instead of 6, the region
+// 11 instead of 10.
+__host__ __device__ inline bool borrow2_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
+                                             int kc1) {
+  const size_t cap = (size_t)(kc0 + kc1);
+  const size_t region = align16((size_t)N * sizeof(double)) + (size_t)arena_bytes;
+  return EMDB_FAST_DIV != 1 && 3 * cap * sizeof(double) <= (size_t)arena_bytes &&
+         11 * cap * sizeof(double) <= region &&
+         (align16((size_t)N * sizeof(double)) + kRedBytes) <= slab_stride;
+}
+
+__device__ __forceinline__ Knots place_knots_borrow2(double* imf, char* arena, int arena_bytes,
+                                                     char* slab, int N, int kc0, int kc1) {
+  Knots K;
+  K.cap = kc0 + kc1;
+  double* p = reinterpret_cast<double*>(arena + arena_bytes) - 3 * K.cap;
+  K.X[0] = p; p += kc0;
+  K.Y[0] = p; p += kc0;
+  K.X[1] = p; p += kc1;
+  K.Y[1] = p; p += kc1;
+  K.M[0] = p;
+  K.M[1] = p + kc0;
+  K.P[0] = imf;
+  K.P[1] = imf + 4 * K.cap;
+  K.R[0] = K.P[1];
+  K.R[1] = K.P[1] + 2 * K.cap;
+  K.red = reinterpret_cast<double*>(slab + align16((size_t)N * sizeof(double)));
+  return K;
+}
+
 // Park placement, for passes whose knots fit neither shared-memory placement
 // but whose PCR buffer 1 fits the proto-IMF's space (long traces with many
 // knots): the proto-IMF is parked in the slab as for the borrow placement,
@@ -341,7 +377,8 @@ __device__ __forceinline__ Knots place_knots_park(double* imf, char* slab, int N
   return K;
 }
 
-enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3, kPlacePark = 4 };
+enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3, kPlacePark = 4,
+              kPlaceBorrow2 = 5 };
 enum : int { kOnChip = -1, kOffChip = -2, kAnyPlace = -3 };
 
 // Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
@@ -1116,7 +1153,8 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   // kOffChip: one instance for the on-chip (shared, borrow) or off-chip
   // (split, park, slab) placements, chosen by `place` at run time.
   const int kPlace = kGroup >= 0 ? kGroup
-                   : kGroup == kOnChip ? (place == kPlaceBorrow ? kPlaceBorrow : kPlaceSmem)
+                   : kGroup == kOnChip ? ((place == kPlaceBorrow || place == kPlaceBorrow2)
+                                              ? kPlaceBorrow : kPlaceSmem)
                    : kGroup == kOffChip ? (place == kPlaceSplit ? kPlaceSplit
                                            : place == kPlacePark ? kPlacePark : kPlaceSlab)
                                         : place;
@@ -1125,7 +1163,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
   Knots K = kPlace == kPlaceSmem    ? place_knots(L.arena, kc0, kc1)
            : kPlace == kPlaceSplit  ? place_knots_split(L.arena, L.arena_bytes, slab, kc0, kc1)
-           : kPlace == kPlaceBorrow ? place_knots_borrow(imf, L.arena, L.arena_bytes, slab, N, kc0, kc1)
+           : kPlace == kPlaceBorrow ? (place == kPlaceBorrow2
+                                          ? place_knots_borrow2(imf, L.arena, L.arena_bytes, slab, N, kc0, kc1)
+                                          : place_knots_borrow(imf, L.arena, L.arena_bytes, slab, N, kc0, kc1))
+           : kPlace == kPlaceBorrow2 ? place_knots_borrow2(imf, L.arena, L.arena_bytes, slab, N, kc0, kc1)
            : kPlace == kPlacePark   ? place_knots_park(imf, slab, N, kc0, kc1, L.red)
                                     : place_knots(slab, kc0, kc1);
   PassSums ps;
@@ -1134,7 +1175,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   bool mbad = false;
   if (warp == 0) {
     mbad = mirror_both(L, K, e, N, NB, T, lane);
-  } else if (kPlace == kPlaceBorrow || kPlace == kPlacePark) {
+  } else if (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark) {
     // park the proto-IMF while warp 0 mirrors; PCR buffer 1 overwrites it
     double* save = borrow_save(slab);
     for (int i = tid - 32; i < N; i += kThreads - 32) save[i] = imf[i];
@@ -1142,7 +1183,8 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   ps.bad = __syncthreads_or(bad || mbad) != 0;
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
   solve_splines<kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid);
-  const double* oldv = (kPlace == kPlaceBorrow || kPlace == kPlacePark) ? borrow_save(slab) : imf;
+  const double* oldv = (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark)
+                            ? borrow_save(slab) : imf;
 
   SideView sv0, sv1;
   sv0.x = K.X[0] + kb0; sv0.y = K.Y[0] + kb0; sv0.M = K.M[0]; sv0.R = K.R[0];
@@ -1389,12 +1431,13 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         {
           const int place = knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSmem
                           : borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlaceBorrow
+                          : borrow2_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlaceBorrow2
                           : split_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSplit
                           : park_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlacePark
                                                                          : kPlaceSlab;
           if (EMDB_MERGED_PLACE == 2)
             flags = sift_pass<kAnyPlace, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
-          else if (place == kPlaceSmem || place == kPlaceBorrow)
+          else if (place == kPlaceSmem || place == kPlaceBorrow || place == kPlaceBorrow2)
             flags = sift_pass<kOnChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
           else
             flags = sift_pass<kOffChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
@@ -1405,6 +1448,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
           flags = sift_pass<kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
         } else if (borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
           flags = sift_pass<kPlaceBorrow, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          ++spilled;
+        } else if (borrow2_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
+          flags = sift_pass<kPlaceBorrow2, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
           ++spilled;
         } else if (split_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
           flags = sift_pass<kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane);

@@ -271,6 +271,26 @@ def test_park_placement_same_results(N, arena):
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("N,arena", [(16384, 232448), (8192, 115712)])
+def test_compact_borrow_same_results(N, arena):
+    """Long traces whose knots need the compact borrow placement (moments
+    beside X | Y at the arena's end, both PCR buffers in the parked proto-IMF's
+    space) give the same bits as with every knot in the slab (smallest
+    arena)."""
+    import torch
+    from cuda_emd import EMDKernelConfig, workloads as W
+    rng = np.random.default_rng(312)
+    X = np.concatenate([W.seismic_batch(3, N, seed=313), W.chirp_trace(rng, N)[None, :]])
+    L = EMDKernelConfig().build()
+    L._plan.set_arena(L._plan.min_arena(N))
+    ref = [o.cpu() for o in L.run(torch.from_numpy(X).cuda(), None)]
+    L._plan.set_arena(arena)
+    out = [o.cpu() for o in L.run(torch.from_numpy(X).cuda(), None)]
+    L.check_status()
+    for a, b in zip(ref, out):
+        assert torch.equal(a, b)
+
+
 def test_arena_too_small_raises():
     import torch
     from cuda_emd import EMDKernelConfig
