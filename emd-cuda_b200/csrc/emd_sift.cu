@@ -1176,7 +1176,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   if (warp == 0) {
     mbad = mirror_both(L, K, e, N, NB, T, lane);
   } else if (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark) {
-    // park the proto-IMF while warp 0 mirrors; PCR buffer 1 overwrites it
+    // park the proto-IMF while warp 0 mirrors; the PCR buffers overwrite it
     double* save = borrow_save(slab);
     for (int i = tid - 32; i < N; i += kThreads - 32) save[i] = imf[i];
   }
