@@ -103,7 +103,15 @@ def cpu_oracle_rate(X: np.ndarray, pool, cores: int, sample: int):
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
-    def __init__(self, index: int, path: str):
+    """nvidia-smi clock and throttle-reason samples every 200 ms while the
+    timed region runs; kept in `path` when one is given, else a temp file."""
+
+    def __init__(self, index: int, path: str | None = None):
+        import tempfile
+        self.temp = path is None
+        if path is None:
+            fd, path = tempfile.mkstemp(prefix="emdb_clocks_", suffix=".csv")
+            os.close(fd)
         self.path = path
         self.proc = None
         try:
@@ -117,8 +125,16 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _discard(self):
+        f = getattr(self, "f", None)
+        if f is not None and not f.closed:
+            f.close()
+        if self.temp and os.path.exists(self.path):
+            os.unlink(self.path)
+
     def stop(self):
         if self.proc is None:
+            self._discard()
             return None
         self.proc.terminate()
         try:
@@ -140,6 +156,8 @@ class ClockSampler:
             for n, v in zip(names, parts[4:8]):
                 if v.lower() == "active":
                     reasons.add(n)
+        if self.temp:
+            os.unlink(self.path)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
@@ -187,6 +205,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--arena", type=int, default=0, help="shared-memory arena per CTA (0 = auto)")
+    ap.add_argument("--clocks-csv", default=None,
+                    help="keep the raw clock samples here ({rank} = rank); default: a temp file")
     ap.add_argument("--variant", type=int, default=0, help="kernel register variant: min CTAs/SM")
     ap.add_argument("--train-traces", type=int, default=200000, help="ragged64k: MLP training set")
     ap.add_argument("--eval-traces", type=int, default=0, help="ragged64k: batch size (0 = 65536)")
@@ -256,8 +276,7 @@ def main():
 
     R.barrier(world)
     torch.cuda.synchronize(dev)
-    clocks = ClockSampler(local, os.path.join(ROOT, "gpurun_out", f"clocks_r{rank}.csv")) \
-        if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else None
+    clocks = ClockSampler(local, a.clocks_csv.replace("{rank}", str(rank)) if a.clocks_csv else None)
     st = torch.cuda.current_stream(dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(a.steps)]

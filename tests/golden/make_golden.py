@@ -9,7 +9,7 @@ signals -- the stock build's IMF rows.  It also stores the envelope-only
 kernel's outputs for one group.  Finally it prints how the NumPy oracle
 compares, so a run log shows the pinning result directly.
 
-Usage: python tests/golden/make_golden.py [--out gpurun_out/golden/ref_golden.npz]
+Usage: python tests/golden/make_golden.py [--out tests/golden/ref_golden.npz]
 """
 from __future__ import annotations
 
@@ -40,7 +40,7 @@ def sha(block: np.ndarray) -> bytes:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "ref_golden.npz"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden", "ref_golden.npz"))
     a = ap.parse_args()
     os.makedirs(os.path.dirname(a.out), exist_ok=True)
     libs = {}

@@ -18,7 +18,7 @@ import pytest
 import cases
 from oracle import emd_oracle as O
 
-IMF_RTOL = 1e-9  # x signal range (north-star tolerance for IMF values)
+IMF_RTOL = 1e-9  # x signal range (the stated tolerance for IMF values)
 
 
 def _sha(block):
