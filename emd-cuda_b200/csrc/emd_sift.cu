@@ -381,6 +381,20 @@ enum : int { kPlaceSmem = 0, kPlaceSplit = 1, kPlaceSlab = 2, kPlaceBorrow = 3, 
               kPlaceBorrow2 = 5 };
 enum : int { kOnChip = -1, kOffChip = -2, kAnyPlace = -3 };
 
+// Where one sift pass keeps its knots and PCR buffers: the first placement
+// that fits, the on-chip ones first (shared, borrow, compact borrow), then
+// split, park, slab.  `arena_bytes` is the knot arena left after the fixed
+// part (control block, scan masks, proto-IMF); the slab always fits.
+__host__ __device__ inline int choose_place(int N, int arena_bytes, size_t slab_stride, int kc0,
+                                            int kc1) {
+  return knot_bytes(kc0, kc1) <= (size_t)arena_bytes ? kPlaceSmem
+       : borrow_fits(N, arena_bytes, slab_stride, kc0, kc1) ? kPlaceBorrow
+       : borrow2_fits(N, arena_bytes, slab_stride, kc0, kc1) ? kPlaceBorrow2
+       : split_bytes(kc0, kc1) <= (size_t)arena_bytes ? kPlaceSplit
+       : park_fits(N, arena_bytes, slab_stride, kc0, kc1) ? kPlacePark
+                                                          : kPlaceSlab;
+}
+
 // Correctly rounded a/b from y = RN(1/b) (Markstein, "Computation of elementary
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 1990):
 // if y is within half an ulp of 1/b and q within one ulp of a/b, then with the
@@ -1429,12 +1443,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         int flags;
 #if EMDB_MERGED_PLACE
         {
-          const int place = knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSmem
-                          : borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlaceBorrow
-                          : borrow2_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlaceBorrow2
-                          : split_bytes(kc0, kc1) <= (size_t)L.arena_bytes ? kPlaceSplit
-                          : park_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1) ? kPlacePark
-                                                                         : kPlaceSlab;
+          const int place = choose_place(N, L.arena_bytes, p.slab_stride, kc0, kc1);
           if (EMDB_MERGED_PLACE == 2)
             flags = sift_pass<kAnyPlace, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
           else if (place == kPlaceSmem || place == kPlaceBorrow || place == kPlaceBorrow2)
@@ -1444,23 +1453,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
           spilled += place != kPlaceSmem;
         }
 #else
-        if (knot_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
-          flags = sift_pass<kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
-        } else if (borrow_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
-          flags = sift_pass<kPlaceBorrow, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
-          ++spilled;
-        } else if (borrow2_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
-          flags = sift_pass<kPlaceBorrow2, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
-          ++spilled;
-        } else if (split_bytes(kc0, kc1) <= (size_t)L.arena_bytes) {
-          flags = sift_pass<kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
-          ++spilled;
-        } else if (park_fits(N, L.arena_bytes, p.slab_stride, kc0, kc1)) {
-          flags = sift_pass<kPlacePark, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
-          ++spilled;
-        } else {
-          flags = sift_pass<kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
-          ++spilled;
+        {
+          const int place = choose_place(N, L.arena_bytes, p.slab_stride, kc0, kc1);
+          if (place == kPlaceSmem)
+            flags = sift_pass<kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          else if (place == kPlaceBorrow)
+            flags = sift_pass<kPlaceBorrow, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          else if (place == kPlaceBorrow2)
+            flags = sift_pass<kPlaceBorrow2, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          else if (place == kPlaceSplit)
+            flags = sift_pass<kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          else if (place == kPlacePark)
+            flags = sift_pass<kPlacePark, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          else
+            flags = sift_pass<kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+          spilled += place != kPlaceSmem;
         }
 #endif
         ++passes;
@@ -1781,6 +1788,12 @@ cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
 }
 
 size_t sift_fixed_smem(int N) { return fixed_bytes(N) + kRedBytes; }
+
+int sift_pass_placement(int N, int arena_total, size_t slab_stride, int kc0, int kc1) {
+  const size_t fixed = fixed_bytes(std::max(N, 1));
+  if (arena_total < 0 || (size_t)arena_total < fixed + kRedBytes + 64) return -1;
+  return choose_place(N, arena_total - (int)fixed, slab_stride, kc0, kc1);
+}
 
 size_t sift_slab_bytes(int max_extrema, int nbsym) {
   int kc = max_extrema + 2 * nbsym + 2;

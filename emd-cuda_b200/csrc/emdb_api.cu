@@ -364,6 +364,20 @@ int emdb_min_arena(int max_n, int* arena_bytes) {
   return EMDB_OK;
 }
 
+int emdb_pass_placement(const emdb_config* cfg, int N, int arena_bytes, int n_max, int n_min,
+                        int* placement) {
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  if (N < 1 || arena_bytes < 0 || n_max < 0 || n_min < 0 || n_max > cfg->max_extrema ||
+      n_min > cfg->max_extrema || !placement)
+    return fail(EMDB_ERR_INVALID, "bad arguments");
+  const int kc0 = n_max + 2 * cfg->nbsym + 2, kc1 = n_min + 2 * cfg->nbsym + 2;
+  *placement = emdb::sift_pass_placement(N, arena_bytes & ~15,
+                                         emdb::sift_slab_bytes(cfg->max_extrema, cfg->nbsym),
+                                         kc0, kc1);
+  return EMDB_OK;
+}
+
 int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, int N,
              double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
              void* stream) {

@@ -88,6 +88,11 @@ struct EnvParams {
 size_t sift_fixed_smem(int N);
 // Worst-case global spill bytes per CTA for a given extrema cap / nbsym.
 size_t sift_slab_bytes(int max_extrema, int nbsym);
+// Knot placement a sift pass takes for a trace of N samples in a CTA arena of
+// arena_total bytes with kc0 / kc1 knot slots per envelope (-1: the trace does
+// not fit the arena).  Values: 0 shared, 1 split, 2 slab, 3 borrow, 4 park,
+// 5 compact borrow.
+int sift_pass_placement(int N, int arena_total, size_t slab_stride, int kc0, int kc1);
 
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream);
 cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream);

@@ -33,7 +33,7 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena",
            "emdb_host_bytes", "emdb_host_register", "emdb_host_unregister",
            "emdb_notify_create", "emdb_notify_reset", "emdb_notify_destroy",
-           "emdb_run_ragged_notify")
+           "emdb_run_ragged_notify", "emdb_pass_placement")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -90,6 +90,19 @@ def load() -> ctypes.CDLL:
             getattr(L, name).restype = I
         _lib = L
         return L
+
+
+PLACEMENTS = {0: "shared", 1: "split", 2: "slab", 3: "borrow", 4: "park", 5: "compact borrow",
+              -1: "does not fit"}
+
+
+def pass_placement(cfg: EmdbConfig, N: int, arena_bytes: int, n_max: int, n_min: int) -> int:
+    """Knot placement of one sift pass (see emdb_pass_placement); no GPU needed."""
+    L = load()
+    out = ctypes.c_int()
+    check(L.emdb_pass_placement(ctypes.byref(cfg), int(N), int(arena_bytes), int(n_max),
+                                int(n_min), ctypes.byref(out)), "emdb_pass_placement")
+    return out.value
 
 
 def last_error() -> str:

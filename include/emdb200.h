@@ -79,6 +79,18 @@ int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_
  * block, EMDKernelConfig.shared_mem_bytes, kernels.py:1273-1275); the
  * autotuner uses it as the floor of its candidates. */
 int emdb_min_arena(int max_n, int* arena_bytes);
+/* Where a sift pass keeps its knots and PCR buffers, for a trace of N samples
+ * in a CTA arena of arena_bytes (as emdb_plan_set_arena takes it) whose
+ * current proto-IMF has n_max maxima and n_min minima (after the max_extrema
+ * cap).  *placement: 0 shared memory; 3 borrow (proto-IMF parked in the
+ * global per-CTA slab, both PCR buffers on-chip); 5 compact borrow (the same
+ * with the moments beside the knots); 1 split (PCR buffer 1 in the slab);
+ * 4 park (PCR buffer 1 in the parked proto-IMF's space, knots and buffer 0
+ * in the slab); 2 slab; -1 the trace does not fit the arena.  Host-only, no
+ * device needed.  No reference counterpart (the reference keeps every knot
+ * in one fixed shared buffer, kernels.py:1273-1275). */
+int emdb_pass_placement(const emdb_config* cfg, int N, int arena_bytes, int n_max, int n_min,
+                        int* placement);
 
 /* Dense batch, the reference's run(): signals [batch, N], T [N] or NULL
  * (= arange(N), already normalised as emd.py:83-88 does), outputs
