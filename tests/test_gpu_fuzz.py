@@ -4,7 +4,7 @@ small max_extrema (overflow and truncation), small max_iteration (the
 iteration cap), few output rows, nbsym 1-3, lengths from 3 to thousands of
 samples, plateaus and exact zeros (the serial-scan path), the integer and the
 general time-axis builds, and tight shared-memory arenas that force every
-knot placement (shared, borrow, split, slab)."""
+knot placement (shared, borrow, compact borrow, split, park, slab)."""
 import hashlib
 
 import numpy as np
