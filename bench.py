@@ -459,7 +459,8 @@ def run_reference(a, rank, world, pool, cores):
         return run_reference_ragged(a, pool, cores)
     X = make_workload(a.workload, 0)
     B, N = X.shape
-    per = min(a.cpu_sample or max(cores * 8, 32), B)
+    # enough traces per step that the pool's dispatch is a small part of it
+    per = min(a.cpu_sample or max(cores * 32, 64), B)
     r, n, wall = cpu_reference_steps(X, pool, cores, a.steps, a.warmup, per)
     pool.close()
     cpu = {"value": round(r, 2), "unit": "signals/s", "cores": cores, "kind": "port",
