@@ -94,9 +94,11 @@ struct DeviceGuard {
 // Choice: the most CTAs (up to the plan's register variant) whose arena holds
 // the trace plus room for ~2 x 96 knots; failing that, still 3 CTAs/SM if
 // that arena holds the trace at all, before fewer.  Measured on B200 with
-// seismic traces: N = 4096 ran 87 ms at 3 CTAs/SM (knot room) vs 108 ms at 4
-// (none); N = 8192 ran 688 ms at 3 CTAs/SM (knots spilled) vs 867 ms at 2:
-// below 12 warps per SM latency hiding collapses.
+// seismic traces: N = 8192 (4,096 traces) 1,121 ms at 3 CTAs/SM vs 1,435 ms
+// at 2 -- below 12 warps per SM latency hiding collapses; N = 2048 (8,192
+// traces) 38.4 ms at 4 vs 42.2 ms at 3; N = 4096 within a few percent either
+// way, depending on the batch (81 vs 99 ms at 3 vs 4 CTAs/SM for 2,048
+// traces, 223 vs 218 ms for 8,192).
 int auto_arena(const emdb_plan* p, int max_n) {
   const int per_sm = 233472;
   const size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
