@@ -1,23 +1,35 @@
 """Benchmark: batched FP64 EMD on B200, one JSON line on rank 0.
 
-Default workload (N=1 GPU): 16,384 seismic-like float64 traces of 2048
-samples (Ricker wavelet * Laplace reflectivity + 5-100 Hz band-limited noise
-at 10 dB SNR, dt = 2 ms), PyEMD-default EMD, MAX_IMFS 16, max_iteration 1000.
-One step = one decomposition of the whole batch.
+Default workload (N=1 GPU): the ragged batch -- 65,536 float64 traces with
+lengths log-uniform in [256, 8192] (60 % seismic-like: Ricker wavelet *
+Laplace reflectivity + 5-100 Hz band-limited noise at 10 dB SNR, dt 2 ms;
+38 % three tones + trend + noise; 2 % linear chirps), CSR layout, PyEMD-
+default EMD, MAX_IMFS 16, max_iteration 1000.  One step = one decomposition of
+the whole batch: traces grouped into length tiers, one persistent sift launch
+per tier, the sequence graph-captured.
 
-  value     signals/s with inputs resident in HBM (device-timed launches)
-  e2e       signals/s through GPUBatchEMD on pinned host buffers: each step
-            copies the traces in, decomposes them in one launch while finished
-            chunks of IMF rows stream back, then copies n_imfs, overflow and
-            the debug rows back and checks overflow
-  roofline  the sift kernel's algorithmic FP64 rate (from the logged sift and
+  value     signals/s of the learned-scheduled step (features + BF16 MLP
+            inference + longest-predicted-first queue per tier + the tier
+            launches), inputs resident in HBM, device-timed
+  plain     the same with FIFO queues; learned.speedup_vs_plain, and the
+            ceiling of any ordering (queue ordered by the true logged cost)
+  e2e       signals/s through RaggedRunner.run_host on pinned host CSR
+            buffers: H2D, the learned step, rows with data gathered and
+            copied back with the counts, every step
+  roofline  the sift launches' algorithmic FP64 rate (from the logged sift and
             extrema counts) against a cuBLAS DGEMM measured in this run, plus
-            its HBM rate against MEASURED_PEAKS.json
-  cpu_baseline  the CPU oracle on a bounded sample, all host cores
+            the HBM rate against MEASURED_PEAKS.json
+  cpu_baseline  the CPU oracle on a bounded random sample, all host cores
+  serve     continuous-batching server under Poisson load: saturation and
+            p50/p99/p99.9 latency at a few offered loads
+
+Other workloads: --workload seismic16k (16,384 x 2048 seismic traces, the
+equal-length head-to-head with the reference kernel), seismic8k, serve, ...
 
 ``--impl reference`` times the reference's algorithm on the host cores (the
 CPU oracle restatement: the reference itself is CUDA-only and its CuPy
-dependency is absent) and prints the same line with impl=reference.
+dependency is absent) and prints the same line with impl=reference; beside
+it, the reference's own kernel on the same GPU (padded to max N).
 
 Multi-GPU (torchrun, --gpus N): traces are independent, so each rank
 decomposes its own batch (weak scaling, no data-path collective); timing is
@@ -40,12 +52,31 @@ sys.path.insert(0, os.path.join(ROOT, "emd-cuda_b200"))
 sys.path.insert(0, ROOT)
 
 METRIC = "EMD signals/s (FP64)"
+# the headline metric: the ragged batch, learned order vs plain, with serving latency beside it
+METRIC_HEADLINE = ("EMD signals/s (FP64) learned-scheduled vs plain on one B200; "
+                   "p50/p99 serve latency")
 # DRAM bytes per trace of emd_sift_kernel, keyed by (N, max_imfs): one ncu
 # capture of the seismic1k launch (1024 traces x 2048 samples) read
 # dram__bytes_read.sum 24.33 MB + dram__bytes_write.sum 240.00 MB.  Inputs and
 # outputs are per trace and the spill slab stays in L2, so a launch's traffic
 # is this figure times its traces.
 NCU_DRAM_BYTES_PER_TRACE = {(2048, 16): 264329984 / 1024}
+# DRAM bytes per sample of the ragged mix's tier launches (None until captured)
+NCU_DRAM_BYTES_PER_SAMPLE_RAGGED = None
+NCU_RAGGED_SOURCE = None
+
+
+def hbm_peak_gbs():
+    """(GB/s, source): MEASURED_PEAKS.json's hbm_gbs, else the pool's fallback."""
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.isfile(pk):
+        try:
+            v = json.load(open(pk)).get("hbm_gbs")
+            if v:
+                return float(v), "MEASURED_PEAKS.json hbm_gbs"
+        except Exception:
+            pass
+    return 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
 WORKLOADS = {
     "seismic16k": dict(n=16384, N=2048, desc="16384 seismic traces x 2048 samples, dt 2 ms"),
     "sinusoid256": dict(n=256, N=1024, desc="256 three-tone traces x 1024 samples"),
@@ -200,7 +231,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="seismic16k", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="ragged64k", choices=list(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=0, help="traces for the CPU leg (0 = auto)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -213,6 +244,10 @@ def main():
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--requests", type=int, default=160, help="serve: requests per load level")
     ap.add_argument("--loads", default="0.1,0.3,0.5,0.7,0.9,1.1", help="serve: offered loads")
+    ap.add_argument("--serve-requests", type=int, default=160,
+                    help="ragged64k: requests per load level of the serving sweep (0 = skip)")
+    ap.add_argument("--serve-loads", default="0.3,0.7,1.1",
+                    help="ragged64k: offered loads of the serving sweep")
     ap.add_argument("--ref-sample", type=int, default=4096,
                     help="reference arm, ragged64k: traces per padded GPU measurement")
     a = ap.parse_args()
@@ -225,9 +260,13 @@ def main():
     # CPU pool first (spawn), before any CUDA context exists.
     pool = None
     want_cpu = (a.impl == "reference" or not a.no_cpu) and rank == 0
-    if want_cpu:
+    # the ragged and serving workloads are generated on the host: every rank
+    # needs a pool for that, sharing the host's cores
+    gen_pool = a.impl == "b200" and a.workload in ("ragged64k", "serve")
+    if want_cpu or gen_pool:
         import multiprocessing as mp
-        pool = mp.get_context("spawn").Pool(cores)
+        pool = mp.get_context("spawn").Pool(cores if rank == 0 and world == 1
+                                            else max(2, cores // max(world, 1)))
 
     if a.impl == "reference":
         run_reference(a, rank, world, pool, cores)
@@ -529,7 +568,7 @@ def run_reference_ragged(a, pool, cores):
     vals, offs = gen_ragged(pool, n_eval, w["lo"], w["hi"], seed=2)
     lens = np.diff(offs)
     rng = np.random.default_rng(12345)
-    per = a.cpu_sample or max(cores * 4, 32)
+    per = a.cpu_sample or max(cores * 2, 32)
     # CPU arm: the oracle over bounded random slices of the batch, all cores
     pick = rng.permutation(n_eval)
     rows = [vals[offs[b]:offs[b + 1]] for b in pick[: per * (a.steps + a.warmup)]]
@@ -549,7 +588,7 @@ def run_reference_ragged(a, pool, cores):
     cpu = {"value": round(r_cpu, 2), "unit": "signals/s", "cores": cores, "kind": "port",
            "sample": f"{a.steps} steps of {per} random traces of the batch (after {a.warmup} "
                      f"warm-up steps), NumPy oracle, {cores} processes, {t_cpu:.1f} s timed"}
-    line = {"impl": "reference", "metric": "EMD signals/s (FP64) ragged batch", "value": cpu["value"],
+    line = {"impl": "reference", "metric": METRIC_HEADLINE, "value": cpu["value"],
             "unit": "signals/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": round(per / max(r_cpu, 1e-9) * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
@@ -628,9 +667,47 @@ def gen_ragged(pool, n: int, lo: int, hi: int, seed: int, chunk: int = 2048):
     return vals, offs
 
 
+def algorithmic_flops_ragged(lens: np.ndarray, n_imfs, dbg_n, dbg_ext) -> float:
+    """algorithmic_flops summed over traces of different lengths."""
+    dn = np.where(dbg_n > 0, dbg_n, 0).astype(np.float64)
+    de = np.where(dbg_ext > 0, dbg_ext, 0).astype(np.float64)
+    L = np.asarray(lens, dtype=np.float64)
+    per_pass = 65.0 * L[:, None] + 20.0 * (de + 8.0)
+    return float((dn * per_pass).sum() + 4.0 * (L * np.asarray(n_imfs, dtype=np.float64)).sum())
+
+
+def _oracle_rows_timed(args):
+    rows, = args
+    sys.path.insert(0, ROOT)
+    from oracle import emd_oracle as O
+    t0 = time.perf_counter()
+    for x in rows:
+        O.emd_signal(x, np.arange(x.shape[0], dtype=np.float64))
+    return len(rows), time.perf_counter() - t0
+
+
+def cpu_ragged_rate(pool, cores: int, vals, offs, per: int, seed: int = 12345):
+    """The oracle on `per` random traces of a CSR batch, all host cores."""
+    rng = np.random.default_rng(seed)
+    B = offs.shape[0] - 1
+    pick = rng.permutation(B)[:per]
+    rows = [vals[offs[b]:offs[b + 1]] for b in pick]
+    parts = [rows[i::cores] for i in range(cores)]
+    t0 = time.perf_counter()
+    res = pool.map(_oracle_rows_timed, [(q,) for q in parts if q])
+    wall = time.perf_counter() - t0
+    n = sum(r[0] for r in res)
+    return n / wall, n, wall, int(sum(r.shape[0] for r in rows))
+
+
 def run_ragged(a, rank, world, pool, cores):
+    """The headline: the ragged batch (65,536 mixed traces) decomposed with
+    length tiers in one graph-captured launch sequence, plain FIFO queues vs
+    the learned longest-predicted-first order (cost model trained here on the
+    plain method's logged counts), plus a short serving sweep."""
     import torch
     from cuda_emd import EMDKernelConfig
+    from cuda_emd import replicas as R
     from cuda_emd import scheduler as S
     from cuda_emd.ragged import RaggedRunner
     w = WORKLOADS["ragged64k"]
@@ -639,66 +716,116 @@ def run_ragged(a, rank, world, pool, cores):
     ev_vals, ev_offs = gen_ragged(pool, n_eval, w["lo"], w["hi"], seed=2 + 1000 * rank)
     tr_vals, tr_offs = gen_ragged(pool, a.train_traces, w["lo"], w["hi"], seed=3 + 1000 * rank)
     gen_s = time.perf_counter() - t0
+    # CPU baseline (rank 0): the oracle on a bounded random sample of the batch
+    cpu = None
+    if pool is not None and rank == 0 and not a.no_cpu:
+        per = a.cpu_sample or max(cores * 8, 64)
+        rate, n, wall, nsamp = cpu_ragged_rate(pool, cores, ev_vals, ev_offs, per)
+        cpu = {"value": round(rate, 3), "unit": "signals/s", "cores": cores, "kind": "port",
+               "sample": f"{n} random traces of the batch ({nsamp} samples), NumPy oracle, "
+                         f"{cores} processes, {wall:.1f} s wall"}
+    # serving sweep requests (single-GPU runs only: the server is one process)
+    serve_traces = gen_requests(pool, a.serve_requests) if a.serve_requests > 0 and world == 1 else None
     if pool is not None:
         pool.close()
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    R.init(world, "nccl", dev)
     cfg = EMDKernelConfig.for_device(local)
     v = torch.from_numpy(ev_vals).to(dev)
     o = torch.from_numpy(ev_offs).to(dev)
+    lens_h = np.diff(ev_offs)
     B = n_eval
     runner = RaggedRunner(cfg, device=local)
+    st = torch.cuda.current_stream(dev)
 
-    def timed(cost, steps, warm):
-        outs = runner.run(v, o, cost=cost, use_graph=True)
-        for _ in range(max(warm - 1, 0)):
-            outs = runner.run(v, o, cost=cost, outs=outs, use_graph=True)
-        torch.cuda.synchronize()
-        st = torch.cuda.current_stream()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for _ in range(steps):
-            outs = runner.run(v, o, cost=cost, outs=outs, use_graph=True)
-        e1.record(st)
-        torch.cuda.synchronize()
+    def timed(arm, steps, warm, clocks=None):
+        """W warm-up and K timed steps of one arm; per-step events around the
+        whole step and around its tier launches (the graph replay)."""
+        outs = None
+        for _ in range(max(warm, 1)):
+            outs = arm(outs)
+        torch.cuda.synchronize(dev)
         runner.check_status()
-        return outs, e0.elapsed_time(e1) * 1e-3 / steps
+        R.barrier(world)
+        torch.cuda.synchronize(dev)
+        sampler = ClockSampler(local, None) if clocks is not None else None
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        t_s, t_e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_s.record(st)
+        for k in range(steps):
+            ev[k][0].record(st)
+            outs = arm(outs, ev[k][1])
+            ev[k][2].record(st)
+        t_e.record(st)
+        torch.cuda.synchronize(dev)
+        R.barrier(world)
+        if sampler is not None:
+            clocks.append(sampler.stop())
+        runner.check_status()
+        total = R.max_over_ranks(t_s.elapsed_time(t_e) * 1e-3, world, dev)
+        launch = [e[1].elapsed_time(e[2]) * 1e-3 for e in ev]
+        return outs, total / steps, statistics.mean(launch)
 
-    # plain: tiers, FIFO inside each tier
-    plain_out, plain_s = timed(None, a.steps, a.warmup)
+    def plain(outs, mark=None):
+        tiers_, orders_ = runner.prepare(v, o, None, offsets_host=ev_offs)     # FIFO queues
+        if mark is not None:
+            mark.record(st)
+        return runner.launch(tiers_, orders_, v, o, outs, use_graph=True)
+
+    clk = []
+    plain_out, plain_s, plain_launch = timed(plain, a.steps, a.warmup, clk)
     plain_copy = [x.clone() for x in plain_out]
-    # labels for the cost model from the plain method on the training set
+    n_imfs_h = plain_copy[1].cpu().numpy()
+    dbg_n_h, dbg_e_h = plain_copy[3].cpu().numpy(), plain_copy[4].cpu().numpy()
+    flops_step = algorithmic_flops_ragged(lens_h, n_imfs_h, dbg_n_h, dbg_e_h)
+
+    # labels for the cost model: the plain method's logged counts on the training set
     tv = torch.from_numpy(tr_vals).to(dev)
     to = torch.from_numpy(tr_offs).to(dev)
     tl0 = time.perf_counter()
-    tr_out = runner.run(tv, to)
-    torch.cuda.synchronize()
+    lab_runner = RaggedRunner(cfg, device=local)
+    tr_out = lab_runner.run(tv, to, offsets_host=tr_offs)
+    torch.cuda.synchronize(dev)
     label_s = time.perf_counter() - tl0
     labels = S.labels_from_debug(tr_out[3], tr_out[1])
-    del tr_out
+    del tr_out, lab_runner
     feats_tr = S.features(tv, to)
     cm = S.CostModel(local, seed=0)
     tt0 = time.perf_counter()
     hist = cm.fit(feats_tr, labels, epochs=a.epochs, batch=4096, lr=1e-3)
-    torch.cuda.synchronize()
+    torch.cuda.synchronize(dev)
     train_s = time.perf_counter() - tt0
-    del tv, to, feats_tr
+    del tv, to, feats_tr, labels
     torch.cuda.empty_cache()
-    # learned order on the evaluation batch (features + BF16 inference inside the timing)
-    lens = o[1:] - o[:-1]
-    fe0 = torch.cuda.Event(enable_timing=True); fe1 = torch.cuda.Event(enable_timing=True)
-    fe0.record()
-    feats = S.features(v, o)
-    fm = torch.cuda.Event(enable_timing=True)
-    fm.record()
-    cost = S.predicted_cost(cm, feats, lens)
-    fe1.record()
-    torch.cuda.synchronize()
-    predict_s = fe0.elapsed_time(fe1) * 1e-3
-    feat_ms, infer_ms = fe0.elapsed_time(fm), fm.elapsed_time(fe1)
-    learned_out, learned_s = timed(cost, a.steps, a.warmup)
+
+    # learned: features + BF16 inference + per-tier order + the launches, every step
+    lens_d = o[1:] - o[:-1]
+
+    def learned(outs, mark=None):
+        feats = S.features(v, o)
+        cost = S.predicted_cost(cm, feats, lens_d)
+        tiers_, orders_ = runner.prepare(v, o, cost, offsets_host=ev_offs)   # device-side order
+        if mark is not None:
+            mark.record(st)
+        return runner.launch(tiers_, orders_, v, o, outs, use_graph=True)
+
+    learned_out, learned_s, learned_launch = timed(learned, a.steps, a.warmup, clk)
     same = all(torch.equal(x, y) for x, y in zip(plain_copy, learned_out))
+    # ceiling: the queue ordered by the TRUE cost (N x logged passes, known only afterwards)
+    true_cost = torch.from_numpy(lens_h * np.maximum(np.where(dbg_n_h > 0, dbg_n_h, 0).sum(1), 1)
+                                 ).to(dev, torch.float32)
+
+    def oracle_order(outs, mark=None):
+        tiers_, orders_ = runner.prepare(v, o, true_cost, offsets_host=ev_offs)
+        if mark is not None:
+            mark.record(st)
+        return runner.launch(tiers_, orders_, v, o, outs, use_graph=True)
+
+    k_true = min(a.steps, 5)
+    _, true_s, _ = timed(oracle_order, k_true, 1)
+    feats = S.features(v, o)
     truth = S.labels_from_debug(plain_copy[3], plain_copy[1])
     pred = cm.predict(feats)
     mae_log2_passes = float((pred[:, 0] - truth[:, 0]).abs().mean())
@@ -706,11 +833,13 @@ def run_ragged(a, rank, world, pool, cores):
     passes_pred = (torch.exp2(pred[:, 0]) - 1).clamp(min=0)
     mae_passes = float((passes_pred - passes_true).abs().mean())
     mae_nimfs = float((pred[:, 1] - truth[:, 1]).abs().mean())
+
+    # per-tier anatomy (each tier alone, learned order)
     tiers = {}
     for t in runner._tiers.values():
         t.plan.counters(reset=True)
-    runner.run(v, o, cost=cost, use_graph=True)
-    torch.cuda.synchronize()
+    runner.run_learned(v, o, cm, use_graph=False, offsets_host=ev_offs)
+    torch.cuda.synchronize(dev)
     for t in runner._tiers.values():
         ps, sp = t.plan.counters(reset=True)
         sub = torch.from_numpy(t.idx.astype(np.int32)).to(dev)
@@ -724,28 +853,108 @@ def run_ragged(a, rank, world, pool, cores):
                               "passes": ps, "spilled_frac": round(sp / max(ps, 1), 4),
                               "alone_ms": round(e0.elapsed_time(e1), 2)}
         del outs
-    value = B / (learned_s + predict_s)
-    line = {
-        "metric": METRIC + " learned-scheduled vs plain", "value": round(value, 2),
-        "unit": "signals/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": round((learned_s + predict_s) * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": "ragged64k", "desc": w["desc"], "batch_per_gpu": B,
-                   "samples": int(ev_offs[-1]), "tiers": tiers, "graph": True},
-        "plain": {"value": round(B / plain_s, 2), "ms_per_step": round(plain_s * 1e3, 3)},
-        "learned": {"value": round(value, 2), "ms_per_step": round(learned_s * 1e3, 3),
-                    "predict_ms": round(predict_s * 1e3, 3), "features_ms": round(feat_ms, 3),
-                    "infer_ms": round(infer_ms, 3),
-                    "speedup_vs_plain": round(plain_s / (learned_s + predict_s), 4),
-                    "bit_identical_to_fifo": bool(same)},
-        "cost_model": {"train_traces": a.train_traces, "epochs": a.epochs,
-                       "loss_first": round(hist[0], 5), "loss_last": round(hist[-1], 5),
-                       "train_s": round(train_s, 3), "label_s": round(label_s, 3),
-                       "mae_log2_passes": round(mae_log2_passes, 4),
-                       "mae_passes": round(mae_passes, 2), "mae_n_imfs": round(mae_nimfs, 4)},
-        "gen_s": round(gen_s, 1), "gpu_launches": a.steps * len(tiers),
-    }
-    print(json.dumps(line), flush=True)
+
+    # end to end through the public API: pinned host CSR in, host results out
+    e2e = None
+    if not a.no_e2e:
+        vals_pin = torch.from_numpy(ev_vals).pin_memory()
+        offs_pin = torch.from_numpy(ev_offs).pin_memory()
+        for _ in range(max(1, min(a.warmup, 2))):
+            runner.run_host(vals_pin, offs_pin, model=cm)
+        torch.cuda.synchronize(dev)
+        R.barrier(world)
+        t_0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(a.steps):
+            res = runner.run_host(vals_pin, offs_pin, model=cm)
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t_0
+        te = R.max_over_ranks(max(e0.elapsed_time(e1) * 1e-3, wall), world, dev)
+        h2d, d2h = runner.last_host_bytes
+        ok = bool(np.array_equal(res.n_imfs.numpy(), n_imfs_h))
+        e2e = {"value": round(R.whole_job_rate(B, a.steps, world, te), 2), "unit": "signals/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "d2h_dense_bytes_per_step": int(8 * cfg.max_imfs * ev_offs[-1]),
+               "api": "cuda_emd.ragged.RaggedRunner.run_host(pinned values, offsets, model=cost model)",
+               "note": "per step: H2D of the CSR traces, features + BF16 inference + learned order, "
+                       "the tier launches, a gather of the rows that may hold data (0..n_imfs), "
+                       "D2H of those rows, counts and debug rows",
+               "n_imfs_equal_device_run": ok}
+        del res
+
+    # roofline of the sift kernel: algorithmic FP64 of one step over the tier launches' time
+    roofline = None
+    if rank == 0:
+        fp64 = dgemm_tflops(dev)
+        achieved = flops_step / learned_launch / 1e12
+        samples = float(ev_offs[-1])
+        hbm_bytes = 8.0 * samples + 8.0 * cfg.max_imfs * samples
+        hbm_peak, hbm_src = hbm_peak_gbs()
+        per_sample = NCU_DRAM_BYTES_PER_SAMPLE_RAGGED
+        roofline = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64, 3),
+                    "unit": "TFLOP/s", "frac": round(achieved / fp64, 4),
+                    "traffic": round(per_sample * samples) if per_sample else None,
+                    "traffic_source": NCU_RAGGED_SOURCE if per_sample else None,
+                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                    "kernel": "emd_sift_kernel (all tier launches of one step)",
+                    "algorithmic_flop_per_launch": flops_step,
+                    "launch_ms": round(learned_launch * 1e3, 3),
+                    "hbm": {"achieved": round(hbm_bytes / learned_launch / 1e9, 1), "peak": hbm_peak,
+                            "unit": "GB/s", "frac": round(hbm_bytes / learned_launch / 1e9 / hbm_peak, 5),
+                            "bytes_per_launch": hbm_bytes, "peak_source": hbm_src}}
+    serve = None
+    if serve_traces:
+        del plain_out, learned_out, plain_copy
+        torch.cuda.empty_cache()
+        serve = serve_sweep(cfg, local, cm, serve_traces,
+                            [float(x) for x in a.serve_loads.split(",")])
+    value = R.whole_job_rate(B, 1, world, learned_s)
+    c = next((x for x in clk if x), None)
+    if c and len(clk) > 1 and clk[1]:
+        c = {"sm_mhz": statistics.median([x["sm_mhz"] for x in clk if x]),
+             "sm_max_mhz": max(x["sm_max_mhz"] for x in clk if x),
+             "reasons": sorted(set(r for x in clk if x for r in x["reasons"])),
+             "samples": sum(x["samples"] for x in clk if x)}
+    if rank == 0:
+        line = {
+            "metric": METRIC_HEADLINE, "value": round(value, 2), "unit": "signals/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(learned_s * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator, see cuda_emd/workloads.py)",
+            "config": {"workload": "ragged64k", "desc": w["desc"], "batch_per_gpu": B,
+                       "samples": int(ev_offs[-1]), "max_imfs": cfg.max_imfs,
+                       "max_extrema": cfg.max_extrema, "max_iteration": cfg.max_iteration,
+                       "queue": "persistent, learned longest-predicted-first per length tier",
+                       "l2": "inputs (1.2 GB) and outputs (19 GB) larger than L2",
+                       "graph": True, "tiers": tiers, "parallelism": f"replicas x{world}"},
+            "plain": {"value": round(R.whole_job_rate(B, 1, world, plain_s), 2),
+                      "ms_per_step": round(plain_s * 1e3, 3),
+                      "launch_ms": round(plain_launch * 1e3, 3), "queue": "FIFO per length tier"},
+            "learned": {"value": round(value, 2), "ms_per_step": round(learned_s * 1e3, 3),
+                        "launch_ms": round(learned_launch * 1e3, 3),
+                        "speedup_vs_plain": round(plain_s / learned_s, 4),
+                        "bit_identical_to_fifo": bool(same),
+                        "speedup_true_cost": round(plain_s / true_s, 4),
+                        "true_cost_ms_per_step": round(true_s * 1e3, 3),
+                        "true_cost_note": "queue ordered by N x the trace's logged sift passes "
+                                          "(known only after decomposing it): the ceiling of any "
+                                          f"ordering on this batch ({k_true} steps)",
+                        "mae_log2_passes": round(mae_log2_passes, 4),
+                        "mae_passes": round(mae_passes, 2), "mae_n_imfs": round(mae_nimfs, 4)},
+            "cost_model": {"train_traces": a.train_traces, "epochs": a.epochs, "batch": 4096,
+                           "lr": 1e-3, "loss_first": round(hist[0], 5), "loss_last": round(hist[-1], 5),
+                           "train_s": round(train_s, 3), "label_s": round(label_s, 3)},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": c, "serve": serve,
+            "gen_s": round(gen_s, 1),
+            "gpu_launches": a.steps * (len(tiers) + 2),
+            "gpu_launches_note": "per learned step: one emd_sift_kernel launch per length tier, "
+                                 "features_kernel, the BF16 MLP inference kernel",
+        }
+        print(json.dumps(line), flush=True)
+    R.finish(world)
 
 
 # ---------------------------------------------------------------------------
@@ -760,17 +969,51 @@ def _gen_requests_chunk(args):
     return [r.traces for r in make_requests(n, rng, lo=lo, hi=hi, max_traces=mt)]
 
 
+def gen_requests(pool, nreq: int, seed0: int = 4000):
+    """The serving workload's requests (trace lists), generated in 8 seeded chunks."""
+    w = WORKLOADS["serve"]
+    parts = [(max(1, -(-nreq // 8)), w["lo"], w["hi"], w["max_traces"], seed0 + k) for k in range(8)]
+    res = pool.map(_gen_requests_chunk, parts) if pool is not None else [_gen_requests_chunk(p) for p in parts]
+    return [t for chunk in res for t in chunk][:nreq]
+
+
+def serve_sweep(cfg, local: int, cm, traces: list, loads: list, slots: int = 4) -> dict:
+    """Continuous-batching server under Poisson arrivals: closed-loop
+    saturation (every request at t=0), then each offered load as a fraction of
+    it; p50/p99/p99.9 latency (delivery - arrival) per level."""
+    from cuda_emd.serving import EMDServer, Request, run_open_loop, poisson_arrivals
+    nreq = len(traces)
+    mk = lambda: [Request(i, trs) for i, trs in enumerate(traces)]
+    # warm-up (plans, kernels) and saturation
+    run_open_loop(EMDServer(cfg, local, slots=slots, cost_model=cm), mk()[:8], np.zeros(8))
+    sat = run_open_loop(EMDServer(cfg, local, slots=slots, cost_model=cm), mk(), np.zeros(nreq))
+    sat_tps = sat["traces_per_s"]
+    mean_tr = sum(len(t) for t in traces) / nreq
+    rng = np.random.default_rng(77)
+    levels = []
+    for load in loads:
+        rate = load * sat_tps / mean_tr
+        arr = poisson_arrivals(rate, nreq, rng)
+        arr -= arr[0]
+        rep = run_open_loop(EMDServer(cfg, local, slots=slots, cost_model=cm), mk(), arr,
+                            timeout_s=900)
+        rep.update({"offered_load": load, "offered_traces_per_s": round(load * sat_tps, 1)})
+        levels.append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in rep.items()})
+    return {"desc": WORKLOADS["serve"]["desc"], "requests_per_level": nreq,
+            "mean_traces_per_request": round(mean_tr, 2), "slots": slots,
+            "order": "learned longest-predicted-first inside each admitted batch",
+            "saturation": {"traces_per_s": round(sat_tps, 1), "p50_ms": round(sat["p50_ms"], 2),
+                           "p99_ms": round(sat["p99_ms"], 2)},
+            "levels": levels}
+
+
 def run_serve(a, rank, world, pool, cores):
     import torch
     from cuda_emd import EMDKernelConfig
     from cuda_emd import scheduler as S
-    from cuda_emd.serving import EMDServer, Request, run_open_loop, poisson_arrivals
     w = WORKLOADS["serve"]
-    nreq = a.requests
     t0 = time.perf_counter()
-    parts = [(max(1, nreq // 8), w["lo"], w["hi"], w["max_traces"], 4000 + k) for k in range(8)]
-    res = pool.map(_gen_requests_chunk, parts) if pool is not None else [_gen_requests_chunk(p) for p in parts]
-    traces = [t for chunk in res for t in chunk][:nreq]
+    traces = gen_requests(pool, a.requests)
     gen_s = time.perf_counter() - t0
     if pool is not None:
         pool.close()
@@ -786,33 +1029,17 @@ def run_serve(a, rank, world, pool, cores):
     cm = S.CostModel(local, seed=0)
     cm.fit(S.features(tvd, tod), S.labels_from_debug(out[3], out[1]), epochs=a.epochs, batch=1024)
     del out, tvd, tod
-    mk = lambda: [Request(i, trs) for i, trs in enumerate(traces)]
-    # warm-up (plans, autotune-free tiers, kernels) and saturation (everything at t=0)
-    srv = EMDServer(cfg, local, slots=4, cost_model=cm)
-    run_open_loop(srv, mk()[:8], np.zeros(8))
-    sat = run_open_loop(EMDServer(cfg, local, slots=4, cost_model=cm), mk(), np.zeros(nreq))
-    sat_tps = sat["traces_per_s"]
-    mean_tr = sum(len(t) for t in traces) / nreq
-    rng = np.random.default_rng(77)
-    levels = []
-    for load in [float(x) for x in a.loads.split(",")]:
-        rate = load * sat_tps / mean_tr
-        arr = poisson_arrivals(rate, nreq, rng)
-        arr -= arr[0]
-        rep = run_open_loop(EMDServer(cfg, local, slots=4, cost_model=cm), mk(), arr, timeout_s=900)
-        rep.update({"offered_load": load, "offered_traces_per_s": round(load * sat_tps, 1)})
-        levels.append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in rep.items()})
+    sv = serve_sweep(cfg, local, cm, traces, [float(x) for x in a.loads.split(",")])
+    levels = sv["levels"]
     p99_90 = next((l["p99_ms"] for l in levels if abs(l["offered_load"] - 0.9) < 1e-6), None)
     line = {
         "metric": "EMD serve latency (FP64)", "value": p99_90, "unit": "ms p99 at 90% load",
         "n_gpus": world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": "serve", "desc": w["desc"], "requests_per_level": nreq,
-                   "mean_traces_per_request": round(mean_tr, 2), "slots": 4,
-                   "order": "learned longest-predicted-first inside each admitted batch"},
-        "saturation": {"traces_per_s": round(sat_tps, 1), "p50_ms": round(sat["p50_ms"], 2),
-                       "p99_ms": round(sat["p99_ms"], 2)},
-        "levels": levels, "gen_s": round(gen_s, 1),
+        "config": {"workload": "serve", "desc": w["desc"], "requests_per_level": sv["requests_per_level"],
+                   "mean_traces_per_request": sv["mean_traces_per_request"], "slots": sv["slots"],
+                   "order": sv["order"]},
+        "saturation": sv["saturation"], "levels": levels, "gen_s": round(gen_s, 1),
     }
     print(json.dumps(line), flush=True)
 

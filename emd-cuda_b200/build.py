@@ -28,6 +28,7 @@ UNITS = [
     ("emd_sched.cu", []),
     ("emdb_api.cu", []),
     ("emdb_noalloc.cu", []),
+    ("emdb_pack.cu", []),
 ]
 HEADERS = ["emdb_internal.cuh", "emdb_sched.cuh"]
 

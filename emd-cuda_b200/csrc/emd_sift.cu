@@ -217,10 +217,11 @@ struct Knots {
 };
 
 __host__ __device__ inline size_t knot_bytes(int kc0, int kc1) {
-  const int cap = kc0 + kc1;
+  // size_t throughout: a host-side size query must not wrap for any int input
+  const size_t cap = (size_t)kc0 + (size_t)kc1;
   // with EMDB_FAST_DIV 1 buffer 1 holds the segment reciprocals during evaluation
-  const size_t red_extra = (EMDB_FAST_DIV != 1 && 4 * cap >= kRedDoubles) ? 0 : kRedBytes;
-  return (size_t)(2 * cap + 8 * cap) * sizeof(double) + red_extra;
+  const size_t red_extra = (EMDB_FAST_DIV != 1 && 4 * cap >= (size_t)kRedDoubles) ? 0 : kRedBytes;
+  return (2 * cap + 8 * cap) * sizeof(double) + red_extra;
 }
 
 __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
@@ -246,7 +247,7 @@ __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
 // moments) in the arena, buffer 1 in the per-CTA global slab.  Evaluation then
 // reads shared memory only, and half of the PCR levels read the slab.
 __host__ __device__ inline size_t split_bytes(int kc0, int kc1) {
-  return (size_t)(6 * (kc0 + kc1)) * sizeof(double);
+  return 6 * ((size_t)kc0 + (size_t)kc1) * sizeof(double);
 }
 
 __device__ __forceinline__ Knots place_knots_split(char* sbase, int sbytes, char* gbase, int kc0,
@@ -279,7 +280,7 @@ __device__ __forceinline__ Knots place_knots_split(char* sbase, int sbytes, char
 // values back from the slab; the reduction lanes go to the slab after them.
 __host__ __device__ inline bool borrow_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
                                             int kc1) {
-  const size_t cap = (size_t)(kc0 + kc1);
+  const size_t cap = (size_t)kc0 + (size_t)kc1;
   const size_t region = align16((size_t)N * sizeof(double)) + (size_t)arena_bytes;
   return EMDB_FAST_DIV != 1 && 6 * cap * sizeof(double) <= (size_t)arena_bytes &&
          10 * cap * sizeof(double) <= region &&
@@ -316,7 +317,7 @@ __device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, in
 // 11 instead of 10.
 __host__ __device__ inline bool borrow2_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
                                              int kc1) {
-  const size_t cap = (size_t)(kc0 + kc1);
+  const size_t cap = (size_t)kc0 + (size_t)kc1;
   const size_t region = align16((size_t)N * sizeof(double)) + (size_t)arena_bytes;
   return EMDB_FAST_DIV != 1 && 3 * cap * sizeof(double) <= (size_t)arena_bytes &&
          11 * cap * sizeof(double) <= region &&
@@ -352,7 +353,7 @@ __device__ __forceinline__ Knots place_knots_borrow2(double* imf, char* arena, i
 // solve.
 __host__ __device__ inline bool park_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
                                           int kc1) {
-  const size_t cap = (size_t)(kc0 + kc1);
+  const size_t cap = (size_t)kc0 + (size_t)kc1;
   const size_t imfb = align16((size_t)N * sizeof(double));
   return EMDB_FAST_DIV != 1 && 4 * cap * sizeof(double) <= imfb + (size_t)arena_bytes &&
          imfb + 6 * cap * sizeof(double) <= slab_stride;
@@ -1796,8 +1797,10 @@ int sift_pass_placement(int N, int arena_total, size_t slab_stride, int kc0, int
 }
 
 size_t sift_slab_bytes(int max_extrema, int nbsym) {
-  int kc = max_extrema + 2 * nbsym + 2;
-  return align16(knot_bytes(kc, kc));
+  const long long kc = (long long)max_extrema + 2LL * nbsym + 2;
+  const size_t cap = (size_t)(2 * kc);
+  const size_t red_extra = (EMDB_FAST_DIV != 1 && 4 * cap >= (size_t)kRedDoubles) ? 0 : kRedBytes;
+  return align16(10 * cap * sizeof(double) + red_extra);
 }
 
 namespace {

@@ -99,25 +99,29 @@ struct DeviceGuard {
 // traces) 38.4 ms at 4 vs 42.2 ms at 3; N = 4096 within a few percent either
 // way, depending on the batch (81 vs 99 ms at 3 vs 4 CTAs/SM for 2,048
 // traces, 223 vs 218 ms for 8,192).
-int auto_arena(const emdb_plan* p, int max_n) {
+int auto_arena_for(int smem_optin, int variant, int nbsym, int max_n) {
   const int per_sm = 233472;
   const size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
   auto share = [&](int want) {
-    int arena = std::min(per_sm / want - 1024, p->smem_optin);
+    int arena = std::min(per_sm / want - 1024, smem_optin);
     // shared memory is allocated in 128-byte units: a 16-byte-rounded share
     // can round up past the SM's capacity and lose a CTA (e.g. 5 per SM)
     return arena & ~127;
   };
-  const size_t knot_room = (size_t)(11 * 2 * (96 + 2 * p->cfg.nbsym + 2)) * sizeof(double);
-  for (int want = p->variant; want >= 1; --want)
+  const size_t knot_room = (size_t)(11 * 2 * (96 + 2 * nbsym + 2)) * sizeof(double);
+  for (int want = variant; want >= 1; --want)
     if ((size_t)share(want) >= fixed + knot_room) {
       if (want >= 3) return share(want);
       break;                                   // would drop below 3 CTAs/SM
     }
-  for (int want = std::min(p->variant, 3); want >= 1; --want)
+  for (int want = std::min(variant, 3); want >= 1; --want)
     if ((size_t)share(want) >= fixed + 64) return share(want);
   const size_t need = fixed + 64;
-  return need <= (size_t)p->smem_optin ? (int)((need + 15) & ~size_t(15)) : 0;
+  return need <= (size_t)smem_optin ? (int)((need + 15) & ~size_t(15)) : 0;
+}
+
+int auto_arena(const emdb_plan* p, int max_n) {
+  return auto_arena_for(p->smem_optin, p->variant, p->cfg.nbsym, max_n);
 }
 
 int arena_for(const emdb_plan* p, int max_n) {
@@ -791,9 +795,20 @@ int emdb_plan_counters(emdb_plan* p, unsigned long long* passes, unsigned long l
   return EMDB_OK;
 }
 
-// Error reporting hook for the no-allocation entry point (emdb_noalloc.cu).
+// Hooks for the other translation units (emdb_noalloc.cu, emdb_pack.cu), not
+// exported: error reporting, the planned path's config check, its arena rule.
 __attribute__((visibility("hidden"))) int emdb_noalloc_fail(int code, const char* msg) {
   return fail(code, msg);
+}
+__attribute__((visibility("hidden"))) int emdb_internal_fail(int code, const char* msg) {
+  return fail(code, msg);
+}
+__attribute__((visibility("hidden"))) int emdb_noalloc_check_config(const emdb_config* c) {
+  return check_config(c);
+}
+__attribute__((visibility("hidden"))) int emdb_noalloc_auto_arena(int smem_optin, int nbsym,
+                                                                  int max_n) {
+  return auto_arena_for(smem_optin, 4, nbsym, max_n);
 }
 
 int emdb_check_division(int mode, long long n, unsigned long long seed,

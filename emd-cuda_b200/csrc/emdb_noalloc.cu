@@ -1,23 +1,26 @@
 // emdb_run_noalloc: the dense sift entry point for callers that cannot
 // allocate device memory.
 //
-// Who needs it: code that runs while a CUDA stream is being captured into a
-// graph (device allocation is not allowed there), services that reserve all
-// device memory up front and forbid allocations on their request path, and
-// hosts whose allocator owns the device (allocating behind its back breaks
-// its accounting).  emdb_run needs a plan, and creating a plan allocates its
-// work-queue ticket, status word and spill slab; this entry point instead
-// uses one file-scope device array as that scratch.
+// Who needs it: services that reserve all device memory up front and forbid
+// allocations on their request path, hosts whose own allocator owns the
+// device (allocating behind its back breaks its accounting), and latency-
+// critical paths that cannot afford cudaMalloc/cudaFree (which may
+// synchronise the device).  emdb_run needs a plan, and creating a plan
+// allocates its work-queue ticket, status word and spill slab; this entry
+// point instead uses one file-scope device array as that scratch.
 //
 // The array is kNoAllocScratchBytes (32 MiB) and lives on every GPU that
 // loads the library until the process exits.  Its first 256 bytes hold the
-// queue ticket and status word (cleared before every launch); the rest is the
-// per-CTA spill slab, which bounds how many CTAs one call runs: a config
-// whose per-CTA slab does not fit even once is rejected.  Every call shares
-// the array, so calls that overlap on the GPU (different streams, or another
-// thread) race on it: serialise them.  The array's device address is looked
-// up once per device, on that device's first call, so make the first call
-// outside any stream capture.
+// queue ticket, the status word and the pass counters; the ticket and
+// counters are cleared before every launch, the status word only by
+// emdb_noalloc_status (so a flag raised by any call stays visible until it is
+// read).  The rest is the per-CTA spill slab, which bounds how many CTAs one
+// call runs: a config whose per-CTA slab does not fit even once is rejected.
+// Every call shares the array, so calls that overlap on the GPU (different
+// streams, or another thread) race on it: serialise them.  The array's device
+// address is looked up once per device, on that device's first call, so make
+// the first call before any stream capture; a cudaDeviceReset between calls
+// is not supported (the module, and with it the array, may move).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,39 +43,48 @@ void* g_addr[kMaxDevices] = {};
 
 }  // namespace
 
-// sets the thread's last-error message (defined in emdb_api.cu, not exported)
+// defined in emdb_api.cu, not exported: set the thread's last-error message;
+// the planned path's config check; its automatic arena rule
 extern "C" __attribute__((visibility("hidden"))) int emdb_noalloc_fail(int code, const char* msg);
+extern "C" __attribute__((visibility("hidden"))) int emdb_noalloc_check_config(const emdb_config* c);
+extern "C" __attribute__((visibility("hidden"))) int emdb_noalloc_auto_arena(int smem_optin, int nbsym,
+                                                                             int max_n);
+
+namespace {
+
+// The array's device address on the current device, looked up on the
+// device's first use (nullptr and an error message on failure).
+void* scratch_base(int* dev_out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    emdb_noalloc_fail(EMDB_ERR_CUDA, "no usable current device");
+    return nullptr;
+  }
+  *dev_out = dev;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_addr[dev]) {
+    void* a = nullptr;
+    if (cudaGetSymbolAddress(&a, g_noalloc_scratch) != cudaSuccess || !a) {
+      emdb_noalloc_fail(EMDB_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+      return nullptr;
+    }
+    g_addr[dev] = a;
+  }
+  return g_addr[dev];
+}
+
+}  // namespace
 
 extern "C" int emdb_run_noalloc(const emdb_config* cfg, const double* signals, const double* T,
                                 int batch, int N, double* imfs, int* n_imfs, int* overflow,
                                 int* dbg_n, int* dbg_extno, int* dbg_nzm, void* stream) {
-  if (!cfg) return emdb_noalloc_fail(EMDB_ERR_INVALID, "config is NULL");
-  if (cfg->nbsym < 1 || cfg->nbsym > emdb::kMaxNbsym || cfg->max_extrema < 4 ||
-      cfg->max_iteration < 1 || cfg->max_imfs < 2 || cfg->max_imfs > emdb::kMaxImfsCap)
-    return emdb_noalloc_fail(EMDB_ERR_INVALID, "invalid config");
-  if (cfg->threads_per_block != emdb::kThreads)
-    return emdb_noalloc_fail(EMDB_ERR_UNSUPPORTED, "threads_per_block must be 128");
+  // the same config rules as a plan (max_extrema in [4, 2^20], nbsym, ...)
+  int rc = emdb_noalloc_check_config(cfg);
+  if (rc) return rc;
   if (batch < 0 || N < 0) return emdb_noalloc_fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
   if (batch == 0) return EMDB_OK;
   if ((N > 0 && (!signals || !imfs)) || !n_imfs || !overflow || !dbg_n || !dbg_extno || !dbg_nzm)
     return emdb_noalloc_fail(EMDB_ERR_INVALID, "NULL buffer");
-
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-    return emdb_noalloc_fail(EMDB_ERR_CUDA, "no usable current device");
-  void* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-      e = cudaGetSymbolAddress(&g_addr[dev], g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        g_addr[dev] = nullptr;
-        return emdb_noalloc_fail(EMDB_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
-      }
-    }
-    base = g_addr[dev];
-  }
 
   const size_t stride = (emdb::sift_slab_bytes(cfg->max_extrema, cfg->nbsym) + 255) & ~size_t(255);
   if (kCtlBytes + stride > kNoAllocScratchBytes)
@@ -81,18 +93,22 @@ extern "C" int emdb_run_noalloc(const emdb_config* cfg, const double* signals, c
                               std::to_string(stride) + " bytes of spill scratch per CTA; the "
                               "no-allocation entry point has " +
                               std::to_string(kNoAllocScratchBytes - kCtlBytes) + " bytes").c_str());
+  int dev = 0;
+  void* base = scratch_base(&dev);
+  if (!base) return EMDB_ERR_CUDA;
   int sms = 0, optin = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  // shared-memory arena: the largest that keeps 4 CTAs resident, else the
-  // smallest that holds the trace
-  const size_t fixed = emdb::sift_fixed_smem(std::max(N, 1));
-  int arena = 0;
-  for (int want = 4; want >= 1 && !arena; --want) {
-    int a = std::min(233472 / want - 1024, optin) & ~15;
-    if ((size_t)a >= fixed + 64) arena = a;
-  }
-  if (!arena) return emdb_noalloc_fail(EMDB_ERR_UNSUPPORTED, "trace length does not fit shared memory");
+  cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess || sms < 1 || optin < 1)
+    return emdb_noalloc_fail(EMDB_ERR_CUDA, "device attribute query failed");
+  // shared-memory arena: the planned path's automatic rule (most resident
+  // CTAs whose arena holds the trace plus room for knots, at least 3 per SM
+  // when the trace fits, 128-byte rounded)
+  const int arena = emdb_noalloc_auto_arena(optin, cfg->nbsym, N);
+  if (arena <= 0 || emdb::sift_fixed_smem(std::max(N, 1)) + 64 > (size_t)arena)
+    return emdb_noalloc_fail(EMDB_ERR_UNSUPPORTED,
+                             ("trace length " + std::to_string(N) +
+                              " does not fit this device's shared memory").c_str());
   int per_sm = 0;
   e = emdb::sift_occupancy(arena, 4, &per_sm);
   if (e != cudaSuccess || per_sm < 1) return emdb_noalloc_fail(EMDB_ERR_CUDA, "occupancy query failed");
@@ -101,7 +117,10 @@ extern "C" int emdb_run_noalloc(const emdb_config* cfg, const double* signals, c
 
   unsigned char* ctl = static_cast<unsigned char*>(base);
   cudaStream_t st = (cudaStream_t)stream;
-  e = cudaMemsetAsync(ctl, 0, kCtlBytes, st);   // queue ticket, status word, counters start at zero
+  // queue ticket (bytes 0-3) and pass counters (8-23) start at zero; the
+  // status word (4-7) keeps earlier flags until emdb_noalloc_status reads it
+  e = cudaMemsetAsync(ctl, 0, 4, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctl + 8, 0, 16, st);
   if (e != cudaSuccess) return emdb_noalloc_fail(EMDB_ERR_CUDA, "clearing the scratch control words failed");
 
   emdb::SiftParams sp{};
@@ -131,5 +150,23 @@ extern "C" int emdb_run_noalloc(const emdb_config* cfg, const double* signals, c
   sp.variant = 4;
   e = emdb::launch_sift(sp, grid, st);
   if (e != cudaSuccess) return emdb_noalloc_fail(EMDB_ERR_CUDA, cudaGetErrorString(e));
+  return EMDB_OK;
+}
+
+extern "C" int emdb_noalloc_status(int* status, void* stream) {
+  if (!status) return emdb_noalloc_fail(EMDB_ERR_INVALID, "status is NULL");
+  *status = 0;
+  int dev = 0;
+  void* base = scratch_base(&dev);
+  if (!base) return EMDB_ERR_CUDA;
+  cudaStream_t st = (cudaStream_t)stream;
+  int* word = reinterpret_cast<int*>(static_cast<unsigned char*>(base) + 4);
+  int h = 0;
+  // read into host memory, then clear; both on `stream`, after the calls on it
+  cudaError_t e = cudaMemcpyAsync(&h, word, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(word, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return emdb_noalloc_fail(EMDB_ERR_CUDA, cudaGetErrorString(e));
+  *status = h;
   return EMDB_OK;
 }

@@ -33,7 +33,8 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_plan_counters", "emdb_run_noalloc", "emdb_run_host", "emdb_min_arena",
            "emdb_host_bytes", "emdb_host_register", "emdb_host_unregister",
            "emdb_notify_create", "emdb_notify_reset", "emdb_notify_destroy",
-           "emdb_run_ragged_notify", "emdb_pass_placement")
+           "emdb_run_ragged_notify", "emdb_pass_placement", "emdb_noalloc_status",
+           "emdb_pack_rows")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -83,6 +84,8 @@ def load() -> ctypes.CDLL:
         L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
         L.emdb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         L.emdb_run_noalloc.argtypes = [ctypes.POINTER(EmdbConfig), P, P, I, I, P, P, P, P, P, P, VP]
+        L.emdb_noalloc_status.argtypes = [ctypes.POINTER(I), VP]
+        L.emdb_pack_rows.argtypes = [P, P, P, P, I, I, P, VP]
         L.emdb_plan_counters.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
                                          ctypes.POINTER(ctypes.c_ulonglong), I]
         L.emdb_check_division.argtypes = [I, ctypes.c_longlong, ctypes.c_ulonglong, P]

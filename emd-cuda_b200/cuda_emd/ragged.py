@@ -204,47 +204,69 @@ class RaggedRunner:
             None, 1, order_dev.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
             dn.data_ptr(), de.data_ptr(), dz.data_ptr(), st), "emdb_run_ragged")
 
-    def prepare(self, values, offsets, cost=None):
+    def prepare(self, values, offsets, cost=None, offsets_host=None):
         """Host-side plan: tiers and per-tier queue orders (device int32).
-        Cached for repeated calls on the same offsets / cost tensors."""
-        import torch
-        key = (offsets.data_ptr(), int(offsets.shape[0]), values.data_ptr(),
-               None if cost is None else cost.data_ptr())
+
+        The tiers, their tuning and one persistent order buffer per tier are
+        cached for repeated calls on the same values / offsets tensors (a
+        captured graph reads those buffers); each call refills the buffers on
+        the current stream: FIFO, or longest `cost` first (cost: per-trace
+        work estimates, device tensor or host array).  ``offsets_host`` (the
+        same offsets in host memory) spares the device read-back."""
+        key = (offsets.data_ptr(), int(offsets.shape[0]), values.data_ptr())
         cached = getattr(self, "_prep", None)
-        if cached is not None and cached[0] == key:
-            return cached[1], cached[2]
-        tiers, orders = self._prepare(values, offsets, cost)
-        self._prep = (key, tiers, orders)
+        if cached is None or cached[0] != key:
+            tiers, idx = self._prepare(values, offsets, offsets_host)
+            orders = [x.clone() for x in idx]
+            self._prep = cached = (key, tiers, idx, orders)
+        _, tiers, idx, orders = cached
+        self._fill_orders(idx, orders, cost, values.device)
         return tiers, orders
 
-    def _prepare(self, values, offsets, cost=None):
+    def _prepare(self, values, offsets, offsets_host=None):
         import torch
-        off_h = offsets.cpu().numpy() if hasattr(offsets, "cpu") else np.asarray(offsets)
+        if offsets_host is not None:
+            off_h = np.asarray(offsets_host)
+        else:
+            off_h = offsets.cpu().numpy() if hasattr(offsets, "cpu") else np.asarray(offsets)
         lengths = np.diff(off_h)
         tiers = self.tiers_for(lengths)
         self.tune(values, offsets, lengths, tiers)
-        orders = []
-        cost_h = None if cost is None else (cost.cpu().numpy() if hasattr(cost, "cpu") else np.asarray(cost))
-        for t in tiers:
-            idx = t.idx
-            if cost_h is not None:
-                idx = idx[np.argsort(-cost_h[idx], kind="stable")]
-            orders.append(torch.from_numpy(idx.astype(np.int32)).to(values.device))
-        if cost_h is not None:
-            # longest tier first already; within equal edges the heavier tier leads
-            pass
-        return tiers, orders
+        idx = [torch.from_numpy(t.idx.astype(np.int32)).to(values.device) for t in tiers]
+        return tiers, idx
 
-    def run(self, values, offsets, cost=None, outs=None, use_graph: bool = False):
-        """Decompose; returns (imfs_csr, n_imfs, overflow, debug_n, debug_extno, debug_nzm)."""
+    @staticmethod
+    def _fill_orders(idx, orders, cost, device) -> None:
+        """Each tier's queue: its traces in index order (FIFO), or sorted by
+        decreasing cost (stable, so equal costs keep index order)."""
         import torch
-        tiers, orders = self.prepare(values, offsets, cost)
+        if cost is None:
+            for i, o in zip(idx, orders):
+                o.copy_(i)
+            return
+        c = cost if isinstance(cost, torch.Tensor) else torch.from_numpy(np.asarray(cost))
+        c = c.to(device=device, dtype=torch.float32)
+        for i, o in zip(idx, orders):
+            perm = torch.argsort(c[i.long()], descending=True, stable=True)
+            o.copy_(i[perm])
+
+    def run(self, values, offsets, cost=None, outs=None, use_graph: bool = False,
+            offsets_host=None):
+        """Decompose; returns (imfs_csr, n_imfs, overflow, debug_n, debug_extno, debug_nzm)."""
+        tiers, orders = self.prepare(values, offsets, cost, offsets_host)
+        return self.launch(tiers, orders, values, offsets, outs, use_graph)
+
+    def launch(self, tiers, orders, values, offsets, outs=None, use_graph: bool = False):
+        """The tier launches for a prepare()d batch, with the queue orders its
+        buffers hold now (graph-captured once per batch if use_graph)."""
+        import torch
         if outs is None:
             outs = self._alloc_out(values, offsets)
         main = torch.cuda.current_stream(values.device)
         if use_graph:
             key = (values.data_ptr(), offsets.data_ptr(), outs[0].data_ptr(),
-                   tuple(int(o.data_ptr()) for o in orders), tuple(t.arena for t in tiers))
+                   tuple(int(o.data_ptr()) for o in orders), tuple(t.arena for t in tiers),
+                   tuple(t.variant for t in tiers))
             if self._graph is None or self._graph_key != key:
                 self._issue(tiers, orders, values, offsets, outs, main)   # warm: allocs outside capture
                 torch.cuda.synchronize()
@@ -257,6 +279,88 @@ class RaggedRunner:
         else:
             self._issue(tiers, orders, values, offsets, outs, main)
         return outs
+
+    def run_learned(self, values, offsets, model, outs=None, use_graph: bool = False,
+                    offsets_host=None):
+        """run() with the queue ordered longest-predicted-first by a cost model
+        (cuda_emd.scheduler.CostModel): features and BF16 inference on the
+        device, per-tier order on the device, then the launches.  Same results
+        as FIFO, bit for bit."""
+        from . import scheduler as S
+        feats = S.features(values, offsets)
+        cost = S.predicted_cost(model, feats, offsets[1:] - offsets[:-1])
+        return self.run(values, offsets, cost=cost, outs=outs, use_graph=use_graph,
+                        offsets_host=offsets_host)
+
+    def run_host(self, values, offsets, model=None, use_graph: bool = True):
+        """Host CSR batch in, host results out (the end-to-end path): copy the
+        traces up (page-locked inputs keep the copy asynchronous), order the
+        queue by `model` if given (else FIFO), decompose, gather the rows that
+        may hold data (rows 0..n_imfs of each trace; every later row is zero)
+        into one buffer, and copy that buffer and the counts back.  Returns a
+        HostRagged; its rows() gives trace b's [n_rows, N_b] block."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        vals_h = values if isinstance(values, torch.Tensor) else torch.from_numpy(np.asarray(values))
+        offs_h = offsets if isinstance(offsets, torch.Tensor) else torch.from_numpy(np.asarray(offsets))
+        total, B = int(vals_h.shape[0]), int(offs_h.shape[0]) - 1
+        mi = self.cfg.max_imfs
+        st = getattr(self, "_host_state", None)
+        if st is None or st["total"] != total or st["B"] != B:
+            st = {"total": total, "B": B,
+                  "v": torch.empty(total, dtype=torch.float64, device=dev),
+                  "o": torch.empty(B + 1, dtype=torch.int64, device=dev),
+                  "packed": torch.empty(mi * total, dtype=torch.float64, device=dev),
+                  "host_rows": torch.empty(0, dtype=torch.float64).pin_memory(),
+                  "counts_h": torch.empty((5, B), dtype=torch.int32).pin_memory(),
+                  "dbg_h": torch.empty((3, B, mi), dtype=torch.int32).pin_memory(),
+                  "rowoff_h": torch.empty(B + 1, dtype=torch.int64).pin_memory(),
+                  "outs": None}
+            self._host_state = st
+            self._prep = None
+            self._graph = self._graph_key = None
+        v, o = st["v"], st["o"]
+        off_np = offs_h.numpy()
+        if st.get("off_np") is None or not np.array_equal(st["off_np"], off_np):
+            # new batch layout in the same buffers: plan (tiers, orders, graph) again
+            st["off_np"] = off_np.copy()
+            self._prep = None
+            self._graph = self._graph_key = None
+        v.copy_(vals_h, non_blocking=True)
+        o.copy_(offs_h, non_blocking=True)
+        if st["outs"] is None:
+            st["outs"] = self._alloc_out(v, o)
+        if model is not None:
+            outs = self.run_learned(v, o, model, outs=st["outs"], use_graph=use_graph,
+                                    offsets_host=off_np)
+        else:
+            outs = self.run(v, o, outs=st["outs"], use_graph=use_graph, offsets_host=off_np)
+        imfs, n_imfs, ovf, dn, de, dz = outs
+        lens = o[1:] - o[:-1]
+        n_rows = torch.clamp(n_imfs + 1, max=mi).to(torch.int32)
+        row_off = torch.zeros(B + 1, dtype=torch.int64, device=dev)
+        torch.cumsum(n_rows.to(torch.int64) * lens, 0, out=row_off[1:])
+        _native.check(_native.load().emdb_pack_rows(
+            imfs.data_ptr(), o.data_ptr(), n_rows.data_ptr(), row_off.data_ptr(), B, mi,
+            st["packed"].data_ptr(), torch.cuda.current_stream(dev).cuda_stream), "emdb_pack_rows")
+        st["rowoff_h"].copy_(row_off, non_blocking=True)
+        counts = st["counts_h"]
+        counts[0].copy_(n_imfs, non_blocking=True)
+        counts[1].copy_(ovf, non_blocking=True)
+        counts[2].copy_(n_rows, non_blocking=True)
+        for k, x in enumerate((dn, de, dz)):
+            st["dbg_h"][k].copy_(x, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        need = int(st["rowoff_h"][-1])
+        if st["host_rows"].shape[0] < need:
+            st["host_rows"] = torch.empty(need, dtype=torch.float64).pin_memory()
+        rows_h = st["host_rows"][:need]
+        rows_h.copy_(st["packed"][:need], non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        self.last_host_bytes = (int(vals_h.numel()) * 8 + (B + 1) * 8,
+                                need * 8 + (B + 1) * 8 + 3 * B * 4 + 3 * B * mi * 4)
+        return HostRagged(rows_h, st["rowoff_h"], off_np, counts[2], counts[0], counts[1],
+                          st["dbg_h"])
 
     def _issue(self, tiers, orders, values, offsets, outs, main):
         import torch
@@ -278,3 +382,24 @@ class RaggedRunner:
                 raise ValueError("a trace did not fit its tier's shared-memory arena")
             if st & _native.STATUS_STALE_ENVELOPE:
                 raise RuntimeError("a sample fell outside the envelope knot span")
+
+
+class HostRagged:
+    """Results of RaggedRunner.run_host, in host memory (views of page-locked
+    buffers that the runner's next run_host call overwrites)."""
+
+    def __init__(self, rows, row_off, offsets, n_rows, n_imfs, overflow, dbg):
+        self.packed = rows              # f64: the rows of every trace, back to back
+        self.row_off = row_off          # int64 [B+1]: trace b's rows start at packed[row_off[b]]
+        self.offsets = np.asarray(offsets)
+        self.n_rows = n_rows            # int32 [B]: rows copied for trace b (later rows are zero)
+        self.n_imfs = n_imfs
+        self.overflow = overflow
+        self.debug = dbg                # int32 [3, B, max_imfs]: debug_n, debug_extno, debug_nzm
+
+    def rows(self, b: int) -> np.ndarray:
+        """Trace b's copied rows as a [n_rows, N_b] array."""
+        n = int(self.offsets[b + 1] - self.offsets[b])
+        k = int(self.n_rows[b])
+        s = int(self.row_off[b])
+        return self.packed[s:s + k * n].numpy().reshape(k, n)

@@ -155,6 +155,16 @@ int emdb_run_ragged_notify(emdb_plan* plan, const double* values, const int64_t*
                            int* dbg_n, int* dbg_extno, int* dbg_nzm, emdb_notify* notify,
                            int n_traces, void* stream);
 
+/* Gather the rows of a ragged launch's output that may hold data into one
+ * dense buffer for the copy back to the host: rows [0, n_rows[b]) of trace b
+ * (imfs + max_imfs*offsets[b], rows of N_b samples) go to packed + row_off[b].
+ * All pointers DEVICE memory; n_rows [batch] (clamped to [0, max_imfs]),
+ * row_off int64 [batch] element offsets.  Rows past n_imfs[b] + 1 are zero,
+ * so n_rows = min(n_imfs + 1, max_imfs) keeps everything.  No reference
+ * counterpart (the reference returns dense [batch, MAX_IMFS, N] only). */
+int emdb_pack_rows(const double* imfs, const int64_t* offsets, const int* n_rows,
+                   const int64_t* row_off, int batch, int max_imfs, double* packed, void* stream);
+
 /* Extrema + mirroring + both envelopes on raw traces, no sift loop
  * (run_envelope_only): max_env/min_env [batch, N], n_extrema [batch, 2],
  * degenerate [batch], knot positions/values [batch, mbuf] each with
@@ -172,22 +182,31 @@ int emdb_plan_counters(emdb_plan* plan, unsigned long long* passes,
                        unsigned long long* spilled, int reset);
 
 /* Dense batch like emdb_run, for callers that cannot allocate device memory:
- * code running under CUDA stream capture (allocation is illegal there),
  * services that reserve all device memory up front and forbid allocations on
- * the request path, hosts whose own allocator owns the device.  No plan is
- * needed: the scratch (work-queue ticket, status word, per-CTA spill slab) is
- * one 32 MiB file-scope device array, held by every GPU that loads the
- * library until the process exits.  The slab bounds how many CTAs a call
+ * the request path, hosts whose own allocator owns the device, and paths that
+ * cannot afford cudaMalloc/cudaFree (which may synchronise the device).  No
+ * plan is needed: the scratch (work-queue ticket, status word, per-CTA spill
+ * slab) is one 32 MiB file-scope device array, held by every GPU that loads
+ * the library until the process exits.  The slab bounds how many CTAs a call
  * runs; a config whose per-CTA slab does not fit the array even once is
- * rejected with EMDB_ERR_UNSUPPORTED.  Runs on the current device,
- * asynchronously on `stream`; the device status word is not reported (check
- * `overflow`; T must already be validated).  Every call shares the array:
- * calls that overlap on the GPU race, so serialise them.  A device's first
- * call looks up the array's address; make it outside any stream capture.
+ * rejected with EMDB_ERR_UNSUPPORTED.  The config is checked by the same rules
+ * as emdb_plan_create, and the arena follows the planned path's automatic
+ * rule.  Runs on the current device, asynchronously on `stream`.  Kernel
+ * status flags (EMDB_STATUS_*: a trace too long for the arena, a sample
+ * outside the knot span as a non-monotone T gives) collect in the array's
+ * status word until emdb_noalloc_status reads them.  Every call shares the
+ * array: calls that overlap on the GPU race, so serialise them.  A device's
+ * first call looks up the array's address; make it before any stream capture.
+ * A cudaDeviceReset between calls is not supported.
  * No counterpart in the reference (its run() always allocates, kernels.py:1353-1363). */
 int emdb_run_noalloc(const emdb_config* cfg, const double* signals, const double* T, int batch,
                      int N, double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                      int* dbg_nzm, void* stream);
+/* Synchronise `stream`, then read and clear the no-allocation entry point's
+ * status word on the current device (EMDB_STATUS_* bits of every call since
+ * the last read) into *status.  Allocates nothing.  No counterpart in the
+ * reference (its flags come back with each call's own buffers, emd.py:95-105). */
+int emdb_noalloc_status(int* status, void* stream);
 
 /* Synchronise `stream`, read and clear the plan's device status word
  * (EMDB_STATUS_* bits) into *status. */

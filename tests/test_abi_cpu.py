@@ -77,3 +77,31 @@ def test_cpu_only_call_fails_loudly():
         pytest.skip("GPU present")
     with pytest.raises(Exception):
         GPUBatchEMD(EMDKernelConfig())(np.zeros((1, 64)))
+
+
+def test_noalloc_checks_config_before_any_device_work():
+    # the no-allocation entry point applies the plan's config rules (max_extrema
+    # in [4, 2^20], nbsym in [1, 8], ...) before it touches the device, so an
+    # out-of-range value is refused here, on a machine without a GPU, with the
+    # same code as emdb_plan_create gives
+    import ctypes
+    from cuda_emd import _native
+    L = _native.load()
+    nul = [None] * 6
+    for c in (_native.EmdbConfig((1 << 20) + 1, 2, 1000, 16, 128),
+              _native.EmdbConfig(429496726, 1, 1000, 16, 128),
+              _native.EmdbConfig(1024, 9, 1000, 16, 128),
+              _native.EmdbConfig(1024, 2, 1000, 65, 128)):
+        rc = L.emdb_run_noalloc(ctypes.byref(c), None, None, 4, 256, *nul, None)
+        assert rc == _native.EMDB_ERR_INVALID, (c.max_extrema, rc)
+    c = _native.EmdbConfig(1024, 2, 1000, 16, 256)
+    assert L.emdb_run_noalloc(ctypes.byref(c), None, None, 4, 256, *nul, None) == \
+        _native.EMDB_ERR_UNSUPPORTED
+
+
+def test_slab_bytes_do_not_wrap():
+    # the largest accepted max_extrema still sizes a positive, monotone slab
+    from cuda_emd import _native
+    cfg = _native.EmdbConfig(1 << 20, 8, 1000, 16, 128)
+    p = _native.pass_placement(cfg, 8192, 76800, 1 << 20, 1 << 20)
+    assert p == 2          # every knot in the slab, never a wrapped "fits"

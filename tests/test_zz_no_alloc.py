@@ -1,15 +1,18 @@
 """The no-allocation entry point, emdb_run_noalloc, through the C ABI.
 
-Some callers cannot allocate device memory: code that runs while a stream is
-being captured into a CUDA graph, services that reserve the whole device up
-front and forbid allocations on their request path, and hosts whose own
-allocator owns the device.  For them the library keeps its sift scratch in
-one file-scope device array instead of a plan.  This file checks that its
-results equal the planned entry point's (emdb_run) bit for bit -- the
+Some callers cannot allocate device memory: services that reserve the whole
+device up front and forbid allocations on their request path, hosts whose own
+allocator owns the device, and paths that cannot afford cudaMalloc/cudaFree
+(they may synchronise the device).  For them the library keeps its sift
+scratch in one file-scope device array instead of a plan.  This file checks
+that its results equal the planned entry point's (emdb_run) bit for bit -- the
 tolerance every parity test here uses -- on two calls in a row (the second
-call reuses the array the first one left behind), and that a config whose
-per-CTA scratch cannot fit the array is refused.  It is named to be
-collected last, and passes alone in a fresh process as well.
+call reuses the array the first one left behind), with the default time axis,
+with a given non-uniform time axis, and on long traces whose sift passes keep
+their knots in the array's spill slab; that the status word is read and
+cleared; and that a config whose per-CTA scratch cannot fit the array is
+refused.  It is named to be collected last, and passes alone in a fresh
+process as well.
 """
 import ctypes
 
@@ -26,26 +29,61 @@ def _outputs_like(ref):
             for r in ref]
 
 
-def test_noalloc_equals_planned_entry_on_two_calls():
+def _two_calls_equal(X, T=None, cfg=None):
     import torch
-    from cuda_emd import EMDKernelConfig, _native, workloads as W
+    from cuda_emd import EMDKernelConfig, _native
     L = _native.load()
-    cfg = EMDKernelConfig()
-    X = torch.from_numpy(np.concatenate([W.seismic_batch(200, 2048, seed=901),
-                                         W.sinusoid_batch(56, 2048, seed=902)])).cuda()
+    cfg = cfg or EMDKernelConfig()
     B, N = X.shape
-    ref = cfg.build().run(X, None)              # emdb_run through a plan
+    ref = cfg.build().run(X, T)                 # emdb_run through a plan
     torch.cuda.synchronize()
     c = cfg.to_c()
     stream = torch.cuda.current_stream().cuda_stream
     for call in range(2):
         outs = _outputs_like(ref)
-        rc = L.emdb_run_noalloc(ctypes.byref(c), X.data_ptr(), None, B, N,
-                                *[o.data_ptr() for o in outs], stream)
+        rc = L.emdb_run_noalloc(ctypes.byref(c), X.data_ptr(), None if T is None else T.data_ptr(),
+                                B, N, *[o.data_ptr() for o in outs], stream)
         assert rc == 0, _native.last_error()
         torch.cuda.synchronize()
         for a, b in zip(ref, outs):
             assert torch.equal(a, b), f"call {call}: no-allocation result differs"
+    st = ctypes.c_int(-1)
+    assert L.emdb_noalloc_status(ctypes.byref(st), stream) == 0, _native.last_error()
+    assert st.value == 0, f"status word {st.value}"
+    return ref
+
+
+def test_noalloc_equals_planned_entry_on_two_calls():
+    import torch
+    from cuda_emd import workloads as W
+    X = torch.from_numpy(np.concatenate([W.seismic_batch(200, 2048, seed=901),
+                                         W.sinusoid_batch(56, 2048, seed=902)])).cuda()
+    _two_calls_equal(X)
+
+
+def test_noalloc_given_time_axis():
+    import torch
+    from cuda_emd import workloads as W
+    from cuda_emd.emd import _normalise_T
+    N = 1536
+    X = torch.from_numpy(W.seismic_batch(64, N, seed=903)).cuda()
+    steps = np.random.default_rng(904).uniform(0.5, 2.0, N - 1)
+    T = np.concatenate([[0.0], np.cumsum(steps)])
+    Tn = _normalise_T(torch.from_numpy(T).cuda(), N, torch.cuda.current_device())
+    _two_calls_equal(X, Tn.contiguous())
+
+
+def test_noalloc_long_traces_use_the_slab():
+    # 8192-sample seismic traces exceed max_extrema: at the automatic arena
+    # (3 CTAs/SM) their passes keep knots and PCR buffers in the spill slab
+    import torch
+    from cuda_emd import EMDKernelConfig, _native, workloads as W
+    cfg = EMDKernelConfig(max_iteration=40)          # keeps the test short
+    X = torch.from_numpy(W.seismic_batch(6, 8192, seed=905)).cuda()
+    arena, _, _ = cfg.build()._plan.query(8192)
+    assert _native.pass_placement(cfg.to_c(), 8192, arena, cfg.max_extrema, cfg.max_extrema) in (2, 4)
+    ref = _two_calls_equal(X, cfg=cfg)
+    assert int(ref[2].sum()) == X.shape[0]           # every trace overflowed
 
 
 def test_noalloc_rejects_oversized_scratch():
