@@ -13,6 +13,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>   // header-only NVTX v3: ranges cost nothing without a profiler
+
 #include "../../include/emdb200.h"
 #include "emdb_internal.cuh"
 
@@ -65,6 +67,13 @@ struct emdb_notify {
 namespace {
 
 thread_local std::string g_last_error;
+
+// NVTX range for the span of a scope (plan, launch and copy steps show up by
+// name on an Nsight timeline; without a tool attached the calls are no-ops)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -266,6 +275,7 @@ int emdb_last_error(char* buf, size_t len) {
 }
 
 int emdb_plan_create(const emdb_config* cfg, int device, emdb_plan** out) {
+  NvtxRange nvtx_range("emdb_plan_create");
   if (!out) return fail(EMDB_ERR_INVALID, "out is NULL");
   *out = nullptr;
   int rc = check_config(cfg);
@@ -387,6 +397,7 @@ int emdb_pass_placement(const emdb_config* cfg, int N, int arena_bytes, int n_ma
 int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, int N,
              double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
              void* stream) {
+  NvtxRange nvtx_range("emdb_run");
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
   if (batch == 0) return EMDB_OK;
@@ -414,6 +425,7 @@ int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, in
 int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batch, int N,
                   double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                   int* dbg_nzm, void* stream) {
+  NvtxRange nvtx_range("emdb_run_host");
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
   if (batch == 0) return EMDB_OK;
@@ -557,6 +569,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   if (e == cudaSuccess) e = cudaEventRecord(p->ev_kernel, st);     // after every group's kernel
   if (e != cudaSuccess) return drain(e, "host-pipeline event");
 
+  NvtxRange nvtx_copyback("emdb_run_host copy-back");
   // Copy each chunk back as soon as its flag is up: only its first `rows`
   // rows per trace (the flag holds 1 + the largest count of rows that may
   // hold data); host threads write the zero rows after them meanwhile.  Once
@@ -627,6 +640,7 @@ static int run_ragged_impl(emdb_plan* p, const double* values, const int64_t* of
                            int max_n, const double* T, int t_per_trace, const int* order,
                            double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                            int* dbg_nzm, emdb_notify* nt, int n_traces, void* stream) {
+  NvtxRange nvtx_range("emdb_run_ragged");
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || max_n < 0) return fail(EMDB_ERR_INVALID, "batch and max_n must be >= 0");
   if (batch == 0) return EMDB_OK;
@@ -730,6 +744,7 @@ int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batc
                   double* max_env, double* min_env, int* n_extrema, int* degenerate,
                   double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
                   int* n_mirrored, void* stream) {
+  NvtxRange nvtx_range("emdb_envelope");
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
   if (batch == 0) return EMDB_OK;

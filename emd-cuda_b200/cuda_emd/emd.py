@@ -10,8 +10,9 @@
 int32, ``last_debug`` holds (debug_n, debug_extno, debug_nzm) [batch, MAX_IMFS].
 Results are returned in the caller's array framework (torch, CuPy or NumPy).
 
-Beyond the reference: ``ragged(values, offsets, order=None)`` decomposes a
-CSR batch of mixed-length traces in one launch.
+Beyond the reference: ``ragged(values, offsets, T=None, order=None)``
+decomposes a CSR batch of mixed-length traces, each with its own time axis
+if given, in one launch.
 """
 from __future__ import annotations
 
@@ -44,6 +45,32 @@ def _normalise_T(T, N: int, device: int):
     dn = Tn[1:] - Tn[:-1]
     if not bool(torch.isfinite(Tn).all()) or not bool((dn > 0).all()):
         raise ValueError("T must normalise to a finite, strictly increasing axis")
+    return Tn
+
+
+def _normalise_T_csr(T, offsets, device: int):
+    """Per-trace _normalise_T of CSR-aligned time axes, on the device:
+    (T_b - T_b[0]) / min(diff(T_b)) for every trace b."""
+    import torch
+    from ._arrays import as_device_f64, as_device_i64
+    Td, _ = as_device_f64(T, device)
+    offs = as_device_i64(offsets, device)
+    if Td.dim() != 1 or Td.shape[0] != int(offs[-1].item()):
+        raise ValueError("T must be 1-D and aligned with values (length offsets[-1])")
+    B = offs.shape[0] - 1
+    lens = offs[1:] - offs[:-1]
+    trace = torch.repeat_interleave(torch.arange(B, device=Td.device), lens)
+    first = Td[offs[:-1]]
+    d = Td[1:] - Td[:-1]
+    # steps that stay inside one trace
+    inner = trace[1:] == trace[:-1]
+    big = torch.full((B,), float("inf"), dtype=torch.float64, device=Td.device)
+    big = big.scatter_reduce(0, trace[1:][inner], d[inner], reduce="amin")
+    step = torch.where(torch.isinf(big), torch.ones_like(big), big)
+    Tn = (Td - first[trace]) / step[trace]
+    dn = Tn[1:] - Tn[:-1]
+    if not bool(torch.isfinite(Tn).all()) or not bool((dn[inner] > 0).all()):
+        raise ValueError("each trace's T must normalise to a finite, strictly increasing axis")
     return Tn
 
 
@@ -111,12 +138,18 @@ class GPUBatchEMD:
         self._overflow_warning(overflow, batch)
         return imfs, n_imfs, overflow
 
-    def ragged(self, values, offsets, order=None, max_n: int | None = None):
+    def ragged(self, values, offsets, T=None, order=None, max_n: int | None = None):
         """Decompose a CSR batch (values f64 [total], offsets int64 [batch+1]) in
-        one launch, T = arange(N_b) per trace.  ``order`` (int32 permutation) only
-        sets the queue order.  Returns (imfs_csr, n_imfs, overflow)."""
+        one launch.  ``T``: None = arange(N_b) per trace; else CSR-aligned time
+        axes (f64 [total], trace b's at T[offsets[b]:offsets[b+1]]), each
+        normalised as emd.py:83-88 does for a single T -- this lifts the
+        reference's one-shared-T restriction (emd.py:28-30).  ``order`` (int32
+        permutation) only sets the queue order.  Returns (imfs_csr, n_imfs,
+        overflow)."""
         launcher = self._get_launcher()
+        Tn = None if T is None else _normalise_T_csr(T, offsets, launcher.device)
         imfs, n_imfs, overflow, dn, de, dz = launcher.run_ragged(values, offsets, order=order,
+                                                                 T=Tn, t_per_trace=True,
                                                                  max_n=max_n)
         self.last_debug = (dn, de, dz)
         launcher.check_status()

@@ -253,8 +253,11 @@ class RaggedRunner:
     def run(self, values, offsets, cost=None, outs=None, use_graph: bool = False,
             offsets_host=None):
         """Decompose; returns (imfs_csr, n_imfs, overflow, debug_n, debug_extno, debug_nzm)."""
-        tiers, orders = self.prepare(values, offsets, cost, offsets_host)
-        return self.launch(tiers, orders, values, offsets, outs, use_graph)
+        import torch
+        with torch.cuda.nvtx.range("ragged plan"):
+            tiers, orders = self.prepare(values, offsets, cost, offsets_host)
+        with torch.cuda.nvtx.range("ragged launch"):
+            return self.launch(tiers, orders, values, offsets, outs, use_graph)
 
     def launch(self, tiers, orders, values, offsets, outs=None, use_graph: bool = False):
         """The tier launches for a prepare()d batch, with the queue orders its
@@ -336,6 +339,7 @@ class RaggedRunner:
         else:
             outs = self.run(v, o, outs=st["outs"], use_graph=use_graph, offsets_host=off_np)
         imfs, n_imfs, ovf, dn, de, dz = outs
+        torch.cuda.nvtx.range_push("ragged copy-back")
         lens = o[1:] - o[:-1]
         n_rows = torch.clamp(n_imfs + 1, max=mi).to(torch.int32)
         row_off = torch.zeros(B + 1, dtype=torch.int64, device=dev)
@@ -357,6 +361,7 @@ class RaggedRunner:
         rows_h = st["host_rows"][:need]
         rows_h.copy_(st["packed"][:need], non_blocking=True)
         torch.cuda.current_stream(dev).synchronize()
+        torch.cuda.nvtx.range_pop()
         self.last_host_bytes = (int(vals_h.numel()) * 8 + (B + 1) * 8,
                                 need * 8 + (B + 1) * 8 + 3 * B * 4 + 3 * B * mi * 4)
         return HostRagged(rows_h, st["rowoff_h"], off_np, counts[2], counts[0], counts[1],

@@ -313,8 +313,11 @@ class EMDServer:
 
     def step(self) -> tuple[int, int]:
         """One scheduler tick: reap finished launches, admit pending requests."""
-        d = self._reap()
-        a = self._admit()
+        import torch
+        with torch.cuda.nvtx.range("serve reap"):
+            d = self._reap()
+        with torch.cuda.nvtx.range("serve admit"):
+            a = self._admit()
         return a, d
 
     def drain(self, timeout_s: float = 600.0) -> None:

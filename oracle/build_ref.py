@@ -26,7 +26,8 @@ recipe does the same job with nvcc:
      iteration cap).
 
 The extracted source never lands in the repository.  Run:
-``python oracle/build_ref.py [--ref /root/reference]``.
+``python oracle/build_ref.py --ref <reference checkout>`` (or set
+``EMDB_REFERENCE_DIR``).
 """
 from __future__ import annotations
 
@@ -40,7 +41,8 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# the reference checkout: --ref, else this environment variable
+DEFAULT_REF = os.environ.get("EMDB_REFERENCE_DIR", "")
 
 DEFAULTS = dict(MAX_EXTREMA=1024, NBSYM=2, MAX_ITERATION=1000, MAX_IMFS=16, THREADS=128,
                 REAL_T="double")

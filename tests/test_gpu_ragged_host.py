@@ -89,3 +89,27 @@ def test_pack_rows_kernel_against_numpy():
         want = imfs[mi * offs[b]: mi * offs[b] + k[b] * n]
         assert np.array_equal(got[row_off[b]: row_off[b] + k[b] * n], want), b
     assert np.isnan(got[-5:]).all()
+
+
+def test_public_ragged_with_per_trace_time_axes():
+    # GPUBatchEMD.ragged with one time axis per trace (each normalised as the
+    # reference normalises its single T) against the oracle per trace
+    import torch
+    from cuda_emd import GPUBatchEMD, workloads as W
+    from oracle import emd_oracle as O
+    vals, offs, _ = W.ragged_mix(16, lo=100, hi=2500, seed=61)
+    rng = np.random.default_rng(62)
+    T = np.empty_like(vals)
+    for b in range(16):
+        n = offs[b + 1] - offs[b]
+        T[offs[b]:offs[b + 1]] = 3.0 + np.concatenate([[0.0], np.cumsum(rng.uniform(0.2, 0.9, n - 1))])
+    emd = GPUBatchEMD()
+    imfs, n_imfs, ovf = emd.ragged(torch.from_numpy(vals).cuda(), torch.from_numpy(offs).cuda(),
+                                   T=torch.from_numpy(T).cuda())
+    imfs, n_imfs = imfs.cpu().numpy(), n_imfs.cpu().numpy()
+    for b in range(16):
+        n = int(offs[b + 1] - offs[b])
+        Tb = O.normalise_T(T[offs[b]:offs[b + 1]], n)
+        r = O.emd_signal(vals[offs[b]:offs[b + 1]], Tb)
+        assert n_imfs[b] == r.n_imfs, b
+        assert np.array_equal(imfs[16 * offs[b]:16 * offs[b + 1]].reshape(16, n), r.imfs), b
