@@ -143,7 +143,6 @@ constexpr int kLocalExtBuf = 64;  // kernels.py:206 (serial-fallback trigger)
 
 struct Ctl {
   int job;
-  int w_max[kWarps], w_min[kWarps], w_zc[kWarps], w_zre[kWarps], w_trig[kWarps];
   int head[2][kMaxNbsym + 1];  // first NB+1 extrema indices per side (0 = max, 1 = min)
   int tail[2][kMaxNbsym + 1];  // tail[q][k] = index of extremum n_q-1-k
   int mlist[4][kMaxNbsym + 1]; // mirrored index lists: lmax, lmin, rmax, rmin
@@ -162,8 +161,11 @@ struct Ctl {
 constexpr int kRedDoubles = 6 * kThreads;
 constexpr size_t kRedBytes = kRedDoubles * sizeof(double);
 
+// Per-warp scan counts (maxima, minima, sign changes, zero-run ends, fallback
+// trigger) live right after the control block: 5 x (warps per CTA) ints.
 struct SmemLayout {
   Ctl* ctl;
+  int* wc;            // [5][NW]: w_max | w_min | w_zc | w_zre | w_trig
   double* red;        // [6][128] between passes (= arena start)
   double* imf;        // [N]
   uint32_t* mmax;     // [nch] ballot masks of the last extrema scan
@@ -176,26 +178,37 @@ struct SmemLayout {
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// NT: threads per CTA (128, or 512 for the wide instance).  kGImf: the
+// proto-IMF lives in the CTA's global slab instead of shared memory (traces
+// longer than shared memory holds); it then takes no shared memory.
+template <int NT = kThreads, bool kGImf = false>
 __host__ __device__ inline size_t fixed_bytes(int N) {
   size_t nch = (size_t)(N + 31) / 32;
-  size_t b = align16(sizeof(Ctl));
-  b += align16((size_t)N * sizeof(double));
+  size_t b = align16(sizeof(Ctl)) + align16(5 * (NT / 32) * sizeof(int));
+  if (!kGImf) b += align16((size_t)N * sizeof(double));
   b += align16(nch * 4) * 2 + align16(nch * 2) * 2;
   return b;
 }
 
-__device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total) {
+template <int NT = kThreads, bool kGImf = false>
+__device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total,
+                                            double* gimf = nullptr) {
   SmemLayout L;
   size_t nch = (size_t)(N + 31) / 32;
   char* p = base;
   L.ctl = reinterpret_cast<Ctl*>(p); p += align16(sizeof(Ctl));
+  L.wc = reinterpret_cast<int*>(p); p += align16(5 * (NT / 32) * sizeof(int));
   L.mmax = reinterpret_cast<uint32_t*>(p); p += align16(nch * 4);
   L.mmin = reinterpret_cast<uint32_t*>(p); p += align16(nch * 4);
   L.pmax = reinterpret_cast<uint16_t*>(p); p += align16(nch * 2);
   L.pmin = reinterpret_cast<uint16_t*>(p); p += align16(nch * 2);
   // the proto-IMF directly ahead of the arena: the borrow placement uses both
   // as one region
-  L.imf = reinterpret_cast<double*>(p); p += align16((size_t)N * sizeof(double));
+  if (kGImf) {
+    L.imf = gimf;
+  } else {
+    L.imf = reinterpret_cast<double*>(p); p += align16((size_t)N * sizeof(double));
+  }
   L.arena = p;
   L.red = reinterpret_cast<double*>(p);
   L.arena_bytes = arena_total - (int)(p - base);
@@ -387,7 +400,13 @@ enum : int { kOnChip = -1, kOffChip = -2, kAnyPlace = -3 };
 // split, park, slab.  `arena_bytes` is the knot arena left after the fixed
 // part (control block, scan masks, proto-IMF); the slab always fits.
 __host__ __device__ inline int choose_place(int N, int arena_bytes, size_t slab_stride, int kc0,
-                                            int kc1) {
+                                            int kc1, bool imf_global = false) {
+  // a proto-IMF in global memory has no shared-memory region to lend: only
+  // the placements that leave it alone
+  if (imf_global)
+    return knot_bytes(kc0, kc1) <= (size_t)arena_bytes ? kPlaceSmem
+         : split_bytes(kc0, kc1) <= (size_t)arena_bytes ? kPlaceSplit
+                                                        : kPlaceSlab;
   return knot_bytes(kc0, kc1) <= (size_t)arena_bytes ? kPlaceSmem
        : borrow_fits(N, arena_bytes, slab_stride, kc0, kc1) ? kPlaceBorrow
        : borrow2_fits(N, arena_bytes, slab_stride, kc0, kc1) ? kPlaceBorrow2
@@ -507,10 +526,12 @@ struct TimeAxis {
 // Extrema: count pass (find_extrema_parallel semantics, kernels.py:231-349,
 // with the serial scan's plateau rule, kernels.py:157-200).
 // ---------------------------------------------------------------------------
+template <int NT>
 __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int warp, int lane) {
+  constexpr int NW = NT / 32;
   const double* imf = L.imf;
   int nch = (N + 31) >> 5;
-  int c0 = (warp * nch) / kWarps, c1 = ((warp + 1) * nch) / kWarps;
+  int c0 = (warp * nch) / NW, c1 = ((warp + 1) * nch) / NW;
   int rmax = 0, rmin = 0, zc = 0, zre = 0;
   bool trig = false;
   // neighbours straight from shared memory (conflict-free consecutive
@@ -555,9 +576,9 @@ __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int wa
   }
   trig = __any_sync(kFull, trig);
   if (lane == 0) {
-    Ctl& C = *L.ctl;
-    C.w_max[warp] = rmax; C.w_min[warp] = rmin;
-    C.w_zc[warp] = zc; C.w_zre[warp] = zre; C.w_trig[warp] = trig ? 1 : 0;
+    int* w = L.wc;
+    w[warp] = rmax; w[NW + warp] = rmin;
+    w[2 * NW + warp] = zc; w[3 * NW + warp] = zre; w[4 * NW + warp] = trig ? 1 : 0;
   }
 }
 
@@ -574,19 +595,22 @@ struct ExtInfo {
 // find_extrema_parallel: without a fallback trigger the zero-crossing count is
 // sign changes only; with one, the serial count adds one per zero run that
 // ends before N (kernels.py:123-143, 273-276).
+template <int NT>
 __device__ __forceinline__ ExtInfo extrema_totals(const SmemLayout& L, int warp, int max_extrema) {
+  constexpr int NW = NT / 32;
   const Ctl& C = *L.ctl;
+  const int* wc = L.wc;
   ExtInfo e;
   e.tot_max = e.tot_min = 0;
   int zc = 0, zre = 0;
   bool trig = false;
   e.off_max = e.off_min = 0;
 #pragma unroll
-  for (int w = 0; w < kWarps; ++w) {
-    if (w < warp) { e.off_max += C.w_max[w]; e.off_min += C.w_min[w]; }
-    e.tot_max += C.w_max[w]; e.tot_min += C.w_min[w];
-    zc += C.w_zc[w]; zre += C.w_zre[w];
-    trig |= C.w_trig[w] != 0;
+  for (int w = 0; w < NW; ++w) {
+    if (w < warp) { e.off_max += wc[w]; e.off_min += wc[NW + w]; }
+    e.tot_max += wc[w]; e.tot_min += wc[NW + w];
+    zc += wc[2 * NW + w]; zre += wc[3 * NW + w];
+    trig |= wc[4 * NW + w] != 0;
   }
   e.trig = trig;
   if (!trig && C.chunk_bad) trig = true;
@@ -600,7 +624,8 @@ __device__ __forceinline__ ExtInfo extrema_totals(const SmemLayout& L, int warp,
 // The reference's parallel scan also falls back when one thread's contiguous
 // chunk (ceil(N/128) samples) holds more than 64 strict maxima or minima.  That
 // can only change n_zer when imf[0] == 0 (leading zero), and only for N > 16384,
-// so it is evaluated in that rare case only.  Ends with a barrier.
+// so it is evaluated in that rare case only.  The chunks are the reference's
+// 128 threads' (threads past 128 of a wider CTA have none).  Ends with a barrier.
 __device__ void chunk_fallback_check(const SmemLayout& L, int N, int tid) {
   Ctl& C = *L.ctl;
   const double* s = L.imf;
@@ -619,15 +644,16 @@ __device__ void chunk_fallback_check(const SmemLayout& L, int N, int tid) {
 
 // One extrema scan = count pass + totals.  Ends after a barrier with every
 // thread holding the same totals.
+template <int NT>
 __device__ __forceinline__ ExtInfo extrema_scan(const SmemLayout& L, int N, int tid, int warp,
                                                 int lane, int max_extrema) {
-  extrema_count(L, N, warp, lane);
+  extrema_count<NT>(L, N, warp, lane);
   if (tid == 0) L.ctl->chunk_bad = 0;
   __syncthreads();
-  ExtInfo e = extrema_totals(L, warp, max_extrema);
+  ExtInfo e = extrema_totals<NT>(L, warp, max_extrema);
   if (N > kThreads * 128 && L.imf[0] == 0.0 && !e.trig) {
     chunk_fallback_check(L, N, tid);
-    e = extrema_totals(L, warp, max_extrema);
+    e = extrema_totals<NT>(L, warp, max_extrema);
   }
   return e;
 }
@@ -636,13 +662,15 @@ __device__ __forceinline__ ExtInfo extrema_scan(const SmemLayout& L, int N, int 
 // Knot fill: compacted true extrema -> X/Y at offset NB (both sides).
 // Returns this thread's "bad envelope sign" vote for true knots.
 // ---------------------------------------------------------------------------
+template <int NT>
 __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots& K,
                                                 const ExtInfo& e, int N, int NB,
                                                 const TimeAxis& T, int warp, int lane) {
+  constexpr int NW = NT / 32;
   Ctl& C = *L.ctl;
   const double* imf = L.imf;
   int nch = (N + 31) >> 5;
-  int c0 = (warp * nch) / kWarps, c1 = ((warp + 1) * nch) / kWarps;
+  int c0 = (warp * nch) / NW, c1 = ((warp + 1) * nch) / NW;
   unsigned lt = (1u << lane) - 1u;
   bool bad = false;
   // one extremum lane: rank it, write its knot, note head / tail indices
@@ -913,7 +941,7 @@ __device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* _
   Pn[3 * cap + r] = dk - alpha * d_left - beta * d_right;
 }
 
-template <bool kInt = false>
+template <int NT, bool kInt = false>
 __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kbase1, int kcnt0,
                                               int kcnt1, int tid) {
   const int m0 = kcnt0 >= 4 ? kcnt0 - 2 : 0;
@@ -924,7 +952,7 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
   const double* x1b = K.X[1] + kbase1;
   const double* y0b = K.Y[0] + kbase0;
   const double* y1b = K.Y[1] + kbase1;
-  for (int r = tid; r < mt; r += kThreads) {
+  for (int r = tid; r < mt; r += NT) {
     const bool s0 = r < m0;
     const int k = s0 ? r : r - m0;
     const double* x = s0 ? x0b : x1b;
@@ -942,8 +970,8 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     const double* __restrict__ Pa = cur ? K.P[1] : K.P[0];
     double* __restrict__ Pn = cur ? K.P[0] : K.P[1];
     // two rows per trip: independent division chains overlap
-    for (int r = tid; r < mt; r += (1 + EMDB_PCR_PAIR) * kThreads) {
-      const int r2 = EMDB_PCR_PAIR ? r + kThreads : mt;
+    for (int r = tid; r < mt; r += (1 + EMDB_PCR_PAIR) * NT) {
+      const int r2 = EMDB_PCR_PAIR ? r + NT : mt;
       {
         const bool s0 = r < m0;
         const int mq = s0 ? m0 : m1;
@@ -958,14 +986,14 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     if (s < m0) fin0 ^= 1;
     if (s < m1) fin1 ^= 1;
     cur ^= 1;
-    // Rows are owned by thread r mod 128, so a level with stride >= 128 reads
+    // Rows are owned by thread r mod NT, so a level with stride >= NT reads
     // and writes only the calling thread's rows: no barrier is needed before
     // the next such level.  Earlier levels read other threads' rows, and the
     // solve below does too, so those transitions keep the barrier.
-    if (s < kThreads || 2 * s >= mmax) __syncthreads();
+    if (s < NT || 2 * s >= mmax) __syncthreads();
   }
   // diagonal solve + end-moment recovery (M[0], M[n-1] by the owners of the end rows)
-  for (int r = tid; r < mt; r += kThreads) {
+  for (int r = tid; r < mt; r += NT) {
     const bool s0 = r < m0;
     const int k = s0 ? r : r - m0;
     const int mq = s0 ? m0 : m1;
@@ -1160,10 +1188,19 @@ __device__ __forceinline__ double eval_seg_int(const SideView& s, double t, int 
 // mirroring, both splines, then the fused envelope / mean / update / partial
 // sums.  kPlace selects where the knots live: shared memory (the common case),
 // split between shared memory and the per-CTA global slab, or the slab alone.
-template <int kGroup, bool kInt>
+//
+// NT > 128 (the wide instance, one long trace per CTA): every thread
+// evaluates samples, but the stop-test sums keep the reference's 128 lanes,
+// each adding its samples in order.  So the proto-IMF is always parked in
+// `park_old` (global, per CTA) while warp 0 mirrors, the evaluation writes the
+// update to imf[] and its quotient diff/new to `qbuf`, and the first 128
+// threads then sum old / new / quotient per lane exactly as accumulate() does.
+template <int NT, int kGroup, bool kInt>
 __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
                                               int N, int NB, const TimeAxis& T, int tid, int warp,
-                                              int lane, int place = kPlaceSmem) {
+                                              int lane, int place = kPlaceSmem,
+                                              double* park_old = nullptr, double* qbuf = nullptr) {
+  constexpr bool kWide = NT > kThreads;
   // kGroup >= 0: one placement, fixed at compile time.  kGroup == kOnChip /
   // kOffChip: one instance for the on-chip (shared, borrow) or off-chip
   // (split, park, slab) placements, chosen by `place` at run time.
@@ -1185,11 +1222,15 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
            : kPlace == kPlacePark   ? place_knots_park(imf, slab, N, kc0, kc1, L.red)
                                     : place_knots(slab, kc0, kc1);
   PassSums ps;
-  bool bad = fill_true_knots(L, K, e, N, NB, T, warp, lane);
+  bool bad = fill_true_knots<NT>(L, K, e, N, NB, T, warp, lane);
   bad = __syncthreads_or(bad);
   bool mbad = false;
   if (warp == 0) {
     mbad = mirror_both(L, K, e, N, NB, T, lane);
+  } else if (kWide) {
+    // park the proto-IMF while warp 0 mirrors: the lanes read the old samples
+    // back after the update (and the PCR buffers may overwrite imf[])
+    for (int i = tid - 32; i < N; i += NT - 32) park_old[i] = imf[i];
   } else if (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark) {
     // park the proto-IMF while warp 0 mirrors; the PCR buffers overwrite it
     double* save = borrow_save(slab);
@@ -1197,8 +1238,9 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   }
   ps.bad = __syncthreads_or(bad || mbad) != 0;
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
-  solve_splines<kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid);
-  const double* oldv = (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark)
+  solve_splines<NT, kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid);
+  const double* oldv = kWide ? park_old
+                     : (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark)
                             ? borrow_save(slab) : imf;
 
   SideView sv0, sv1;
@@ -1252,10 +1294,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     const double t0 = T(0), tN = T(N - 1);
     oor = (t0 < sv0.x[0]) || (tN > sv0.x[sv0.n - 1]) || (t0 < sv1.x[0]) || (tN > sv1.x[sv1.n - 1]);
   }
-  // two samples per trip (i, i+128): independent evaluation chains overlap;
+  // two samples per trip (i, i+NT): independent evaluation chains overlap;
   // each lane still accumulates its samples in increasing order
-  for (int i = tid; i < N; i += (1 + EMDB_EVAL_PAIR) * kThreads) {
-    const int i2 = i + kThreads;
+  for (int i = tid; i < N; i += (1 + EMDB_EVAL_PAIR) * NT) {
+    const int i2 = i + NT;
     const bool has2 = EMDB_EVAL_PAIR && i2 < N;
     const double t = T(i);
     const double t2 = has2 ? T(i2) : t;
@@ -1292,6 +1334,14 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     const double emax2 = eval_seg(sv0, t2, lo0b);
     const double emin2 = eval_seg(sv1, t2, lo1b);
 #endif
+    if (kWide) {
+      // the update, and accumulate()'s quotient from the same operands
+      const double old = oldv[i];
+      const double nw = old - 0.5 * (emax + emin);
+      imf[i] = nw;
+      qbuf[i] = (nw - old) / nw;
+      continue;
+    }
     {
       const double mean = 0.5 * (emax + emin);
       const double old = oldv[i];
@@ -1307,15 +1357,33 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       accumulate(ps, old, nw);
     }
   }
+  if (kWide) {
+    // the reference's 128 lanes, each summing its samples in increasing order
+    __syncthreads();
+    if (tid < kThreads) {
+      for (int i = tid; i < N; i += kThreads) {
+        const double old = oldv[i], nw = imf[i], qd = qbuf[i];
+        const double diff = nw - old;
+        ps.sq += nw * nw;
+        ps.dsq += diff * diff;
+        ps.osq += old * old;
+        ps.std_ += qd * qd;
+        ps.omax = fmax(ps.omax, old);
+        ps.omin = fmin(ps.omin, old);
+      }
+    }
+  }
   // per-lane partial sums, then the reference's 128-lane trees on warp 0
   double* red = kPlace == kPlaceSlab ? L.red : K.red;
-  red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
-  red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
+  if (!kWide || tid < kThreads) {
+    red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
+    red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
+  }
   __syncthreads();
 #if EMDB_TREE_SPLIT
   // the six trees spread over the warps (warp w: sum w; warps 0/1 also the
   // max / min tree); the next extrema scan's barrier publishes C.sums
-  {
+  if (!kWide || warp < kWarps) {
     const double a = lane_tree(red + 128 * warp, lane, 0);
     if (lane == 0) C.sums[warp] = a;
     if (warp < 2) {
@@ -1367,16 +1435,27 @@ __device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int 
   }
 }
 
-// kMinBlocks is the register-budget variant: the compiler fits the kernel
-// into 65536 / (128 * kMinBlocks) registers so that many CTAs can be resident.
-template <int kMinBlocks, bool kInt>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftParams p) {
+// NT threads per CTA: 128 (the reference's lanes), or 512 for the wide
+// instance that gives one long trace a whole SM.  kMinBlocks is the
+// register-budget variant: the compiler fits the kernel into
+// 65536 / (NT * kMinBlocks) registers so that many CTAs can be resident.
+// kGImf (wide only): the proto-IMF in the global slab, for traces longer than
+// shared memory holds.
+template <int NT, int kMinBlocks, bool kInt, bool kGImf = false>
+__global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) {
+  constexpr bool kWide = NT > kThreads;
+  static_assert(!kGImf || kWide, "the global proto-IMF is built for the wide instance");
   extern __shared__ __align__(16) char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int NB = p.nbsym;
   const int MAXI = p.max_imfs;
   Ctl* Cs = reinterpret_cast<Ctl*>(smem);
   char* slab = p.slab + (size_t)blockIdx.x * p.slab_stride;
+  // wide instance: the parked proto-IMF and the stop-test quotients (and the
+  // proto-IMF itself for kGImf), past the knot slab in this CTA's stride
+  double* park_old = kWide ? reinterpret_cast<double*>(slab + p.park_off) : nullptr;
+  double* qbuf = kWide ? reinterpret_cast<double*>(slab + p.q_off) : nullptr;
+  double* gimf = kGImf ? reinterpret_cast<double*>(slab + p.imf_off) : nullptr;
 
   for (;;) {
     if (tid == 0) Cs->job = atomicAdd(p.queue, 1);
@@ -1392,14 +1471,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
     T.arange = p.t_mode == kTArange;
     T.T = p.t_mode == kTShared ? p.T : (p.t_mode == kTPerTrace ? p.T + off : nullptr);
 
-    if (fixed_bytes(N) + kRedBytes + 64 > (size_t)p.arena_bytes) {
+    if (fixed_bytes<NT, kGImf>(N) + kRedBytes + 64 > (size_t)p.arena_bytes ||
+        (kWide && p.q_off + (size_t)N * sizeof(double) > p.slab_stride) ||
+        (kGImf && p.imf_off + (size_t)N * sizeof(double) > p.slab_stride)) {
       // cannot hold this trace: report, leave outputs flagged
       if (tid == 0) {
         atomicOr(p.status, kStatusTooLong);
         p.n_imfs[b] = 0;
         p.overflow[b] = 1;
       }
-      for (int k = tid; k < MAXI; k += kThreads) {
+      for (int k = tid; k < MAXI; k += NT) {
         p.dbg_n[(int64_t)b * MAXI + k] = -1;
         p.dbg_ext[(int64_t)b * MAXI + k] = -1;
         p.dbg_nzm[(int64_t)b * MAXI + k] = -1;
@@ -1408,11 +1489,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
       mark_trace_done(p, b, tid, MAXI);     // rows unwritten: the host copies them all
       continue;
     }
-    SmemLayout L = carve(smem, N, p.arena_bytes);
+    SmemLayout L = carve<NT, kGImf>(smem, N, p.arena_bytes, gimf);
     Ctl& C = *L.ctl;
     double* imf = L.imf;
-    for (int k = tid; k < MAXI; k += kThreads) { C.dbg_n[k] = -1; C.dbg_e[k] = -1; C.dbg_z[k] = -1; }
-    for (int i = tid; i < N; i += kThreads) imf[i] = S[i];
+    for (int k = tid; k < MAXI; k += NT) { C.dbg_n[k] = -1; C.dbg_e[k] = -1; C.dbg_z[k] = -1; }
+    for (int i = tid; i < N; i += NT) imf[i] = S[i];
     __syncthreads();
 
     bool ovf = false;
@@ -1422,7 +1503,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
     bool stale = false;
     unsigned long long passes = 0, spilled = 0;
 
-    ExtInfo e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
+    ExtInfo e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
     ovf |= e.overflow;
 
     while (!finished && imf_count < MAXI - 1) {
@@ -1444,30 +1525,43 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         int flags;
 #if EMDB_MERGED_PLACE
         {
-          const int place = choose_place(N, L.arena_bytes, p.slab_stride, kc0, kc1);
+          // the wide instance's stride also holds the parked proto-IMF and the
+          // quotients: its knots may use only the part before them
+          const int place = choose_place(N, L.arena_bytes, kWide ? p.park_off : p.slab_stride,
+                                         kc0, kc1, kGImf);
           if (EMDB_MERGED_PLACE == 2)
-            flags = sift_pass<kAnyPlace, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
+            flags = sift_pass<NT, kAnyPlace, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place,
+                                                   park_old, qbuf);
           else if (place == kPlaceSmem || place == kPlaceBorrow || place == kPlaceBorrow2)
-            flags = sift_pass<kOnChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
+            flags = sift_pass<NT, kOnChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place,
+                                                 park_old, qbuf);
           else
-            flags = sift_pass<kOffChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place);
+            flags = sift_pass<NT, kOffChip, kInt>(L, slab, e, N, NB, T, tid, warp, lane, place,
+                                                  park_old, qbuf);
           spilled += place != kPlaceSmem;
         }
 #else
         {
-          const int place = choose_place(N, L.arena_bytes, p.slab_stride, kc0, kc1);
+          const int place = choose_place(N, L.arena_bytes, kWide ? p.park_off : p.slab_stride,
+                                         kc0, kc1, kGImf);
           if (place == kPlaceSmem)
-            flags = sift_pass<kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+            flags = sift_pass<NT, kPlaceSmem, kInt>(L, slab, e, N, NB, T, tid, warp, lane,
+                                                    place, park_old, qbuf);
           else if (place == kPlaceBorrow)
-            flags = sift_pass<kPlaceBorrow, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+            flags = sift_pass<NT, kPlaceBorrow, kInt>(L, slab, e, N, NB, T, tid, warp, lane,
+                                                      place, park_old, qbuf);
           else if (place == kPlaceBorrow2)
-            flags = sift_pass<kPlaceBorrow2, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+            flags = sift_pass<NT, kPlaceBorrow2, kInt>(L, slab, e, N, NB, T, tid, warp, lane,
+                                                       place, park_old, qbuf);
           else if (place == kPlaceSplit)
-            flags = sift_pass<kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+            flags = sift_pass<NT, kPlaceSplit, kInt>(L, slab, e, N, NB, T, tid, warp, lane,
+                                                     place, park_old, qbuf);
           else if (place == kPlacePark)
-            flags = sift_pass<kPlacePark, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+            flags = sift_pass<NT, kPlacePark, kInt>(L, slab, e, N, NB, T, tid, warp, lane,
+                                                    place, park_old, qbuf);
           else
-            flags = sift_pass<kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane);
+            flags = sift_pass<NT, kPlaceSlab, kInt>(L, slab, e, N, NB, T, tid, warp, lane,
+                                                    place, park_old, qbuf);
           spilled += place != kPlaceSmem;
         }
 #endif
@@ -1475,7 +1569,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         const bool pass_bad = (flags & 1) != 0;
         stale |= (flags & 2) != 0;
         // ---- post-update extrema scan (also next pass's pre-scan) ----
-        e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
+        e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
         ovf |= e.overflow;
         const int extNo2 = e.n_max + e.n_min;
         const int nzm2 = e.n_zer;
@@ -1501,7 +1595,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
         double* row = out + (int64_t)imf_count * N;
         double* rnext = out + (int64_t)(imf_count + 1) * N;
         double gmax = -1e30, gmin = 1e30, gabs = 0.0;
-        for (int i = tid; i < N; i += kThreads) {
+        // the reference's 128 lanes (a wider CTA's other threads wait: once per IMF)
+        for (int i = tid; i < (!kWide || tid < kThreads ? N : 0); i += kThreads) {
           double r = rsrc[i];
           double v = imf[i];
           row[i] = v;
@@ -1512,7 +1607,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
           gabs += fabs(rn);
         }
         double* red = L.red;
-        red[tid] = gmax; red[128 + tid] = gmin; red[256 + tid] = gabs;
+        if (!kWide || tid < kThreads) { red[tid] = gmax; red[128 + tid] = gmin; red[256 + tid] = gabs; }
         __syncthreads();
         if (warp == 0) {
           double a0 = lane_tree(red, lane, 1);
@@ -1526,9 +1621,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
       }
       if (!finished && imf_count < MAXI - 1) {
         const double* rsrc = out + (int64_t)imf_count * N;
-        for (int i = tid; i < N; i += kThreads) imf[i] = rsrc[i];
+        for (int i = tid; i < N; i += NT) imf[i] = rsrc[i];
         __syncthreads();
-        e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
+        e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
         ovf |= e.overflow;
       }
     }
@@ -1539,13 +1634,13 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
     if (trend) imf_count -= 1;
     const double* rres = last_row == 0 ? S : out + (int64_t)last_row * N;
     double amax = 0.0;
-    for (int i = tid; i < N; i += kThreads) {
+    for (int i = tid; i < (!kWide || tid < kThreads ? N : 0); i += kThreads) {
       double r = rres[i];
       if (trend) r = r + imf[i];
       amax = fmax(amax, fabs(r));
     }
     double* red = L.red;
-    red[tid] = amax;
+    if (!kWide || tid < kThreads) red[tid] = amax;
     __syncthreads();
     if (warp == 0) {
       double a = lane_tree(red, lane, 1);
@@ -1554,7 +1649,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
     __syncthreads();
     const bool rzero = C.sums[0] <= kResidueZeroAtol;
     const int nim = rzero ? imf_count : imf_count + 1;
-    for (int i = tid; i < N; i += kThreads) {
+    for (int i = tid; i < N; i += NT) {
       if (trend) {
         double r = rres[i] + imf[i];
         if (!rzero) out[(int64_t)imf_count * N + i] = r;
@@ -1565,7 +1660,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
       }
     }
     const int first_zero = last_row + 1;
-    for (int64_t k = (int64_t)first_zero * N + tid; k < (int64_t)MAXI * N; k += kThreads) out[k] = 0.0;
+    for (int64_t k = (int64_t)first_zero * N + tid; k < (int64_t)MAXI * N; k += NT) out[k] = 0.0;
     if (tid == 0) {
       p.n_imfs[b] = nim;
       p.overflow[b] = ovf ? 1 : 0;
@@ -1575,7 +1670,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) emd_sift_kernel(SiftPara
       }
     }
     if (stale) atomicOr(p.status, kStatusStaleEnvelope);
-    for (int k = tid; k < MAXI; k += kThreads) {
+    for (int k = tid; k < MAXI; k += NT) {
       p.dbg_n[(int64_t)b * MAXI + k] = C.dbg_n[k];
       p.dbg_ext[(int64_t)b * MAXI + k] = C.dbg_e[k];
       p.dbg_nzm[(int64_t)b * MAXI + k] = C.dbg_z[k];
@@ -1602,12 +1697,12 @@ __device__ __forceinline__ void envelope_pass(const SmemLayout& L, char* slab, c
   Ctl& C = *L.ctl;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
   Knots K = place_knots(kSmem ? L.arena : slab, kc0, kc1);
-  fill_true_knots(L, K, e, N, NB, T, warp, lane);
+  fill_true_knots<kThreads>(L, K, e, N, NB, T, warp, lane);
   __syncthreads();
   if (warp == 0) mirror_both(L, K, e, N, NB, T, lane);
   __syncthreads();
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
-  solve_splines(K, kb0, kb1, kn0, kn1, tid);
+  solve_splines<kThreads>(K, kb0, kb1, kn0, kn1, tid);
   SideView sv[2];
   sv[0].x = K.X[0] + kb0; sv[0].y = K.Y[0] + kb0; sv[0].M = K.M[0]; sv[0].R = K.R[0]; sv[0].n = kn0;
   sv[0].nl = NB - kb0; sv[0].nt = e.n_max;
@@ -1668,10 +1763,10 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
       __syncthreads();
       continue;
     }
-    SmemLayout L = carve(smem, N, p.arena_bytes);
+    SmemLayout L = carve<kThreads>(smem, N, p.arena_bytes);
     for (int i = tid; i < N; i += kThreads) L.imf[i] = S[i];
     __syncthreads();
-    ExtInfo e = extrema_scan(L, N, tid, warp, lane, p.max_extrema);
+    ExtInfo e = extrema_scan<kThreads>(L, N, tid, warp, lane, p.max_extrema);
     const bool degenerate = !(e.n_max + e.n_min > 2 && e.n_max >= 1 && e.n_min >= 1);
     int nk[2] = {0, 0};
     if (!degenerate) {
@@ -1788,7 +1883,11 @@ cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
   return cudaGetLastError();
 }
 
-size_t sift_fixed_smem(int N) { return fixed_bytes(N) + kRedBytes; }
+size_t sift_fixed_smem(int N, int variant, bool imf_global) {
+  if (variant_threads(variant) <= kThreads) return fixed_bytes(N) + kRedBytes;
+  return (imf_global ? fixed_bytes<kWideThreads, true>(N) : fixed_bytes<kWideThreads>(N)) +
+         kRedBytes;
+}
 
 int sift_pass_placement(int N, int arena_total, size_t slab_stride, int kc0, int kc1) {
   const size_t fixed = fixed_bytes(std::max(N, 1));
@@ -1806,53 +1905,60 @@ size_t sift_slab_bytes(int max_extrema, int nbsym) {
 namespace {
 // kInt: the kernel build for the integer time axis (T = arange), whose
 // segment quotients use the reciprocal table.
-template <int V, bool kInt>
+template <int NT, int V, bool kInt, bool kG = false>
 cudaError_t occupancy_vt(int arena_bytes, int* ctas_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V, kInt>,
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<NT, V, kInt, kG>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, arena_bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, emd_sift_kernel<V, kInt>,
-                                                       kThreads, arena_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm,
+                                                       emd_sift_kernel<NT, V, kInt, kG>, NT,
+                                                       arena_bytes);
 }
 // CTAs per SM that both builds reach (the smaller), so a plan's grid fits either
-template <int V>
+template <int NT, int V, bool kG = false>
 cudaError_t occupancy_v(int arena_bytes, int* ctas_per_sm) {
   int a = 0, b = 0;
-  cudaError_t e = occupancy_vt<V, true>(arena_bytes, &a);
-  if (e == cudaSuccess) e = occupancy_vt<V, false>(arena_bytes, &b);
+  cudaError_t e = occupancy_vt<NT, V, true, kG>(arena_bytes, &a);
+  if (e == cudaSuccess) e = occupancy_vt<NT, V, false, kG>(arena_bytes, &b);
   *ctas_per_sm = a < b ? a : b;
   return e;
 }
-template <int V, bool kInt>
+template <int NT, int V, bool kInt, bool kG = false>
 cudaError_t launch_vt(const SiftParams& p, int grid, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<V, kInt>,
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<NT, V, kInt, kG>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, p.arena_bytes);
   if (e != cudaSuccess) return e;
-  emd_sift_kernel<V, kInt><<<grid, kThreads, p.arena_bytes, stream>>>(p);
+  emd_sift_kernel<NT, V, kInt, kG><<<grid, NT, p.arena_bytes, stream>>>(p);
   return cudaGetLastError();
 }
-template <int V>
+template <int NT, int V, bool kG = false>
 cudaError_t launch_v(const SiftParams& p, int grid, cudaStream_t stream) {
-  return p.t_mode == kTArange ? launch_vt<V, true>(p, grid, stream)
-                              : launch_vt<V, false>(p, grid, stream);
+  return p.t_mode == kTArange ? launch_vt<NT, V, true, kG>(p, grid, stream)
+                              : launch_vt<NT, V, false, kG>(p, grid, stream);
 }
 }  // namespace
 
-bool sift_variant_ok(int v) { return v == 4 || v == 5 || v == 6; }
+bool sift_variant_ok(int v) { return v == 1 || v == 4 || v == 5 || v == 6; }
 
-cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm) {
+int variant_threads(int v) { return v == 1 ? kWideThreads : kThreads; }
+
+cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm, bool imf_global) {
   switch (variant) {
-    case 5: return occupancy_v<5>(arena_bytes, ctas_per_sm);
-    case 6: return occupancy_v<6>(arena_bytes, ctas_per_sm);
-    default: return occupancy_v<4>(arena_bytes, ctas_per_sm);
+    case 1: return imf_global ? occupancy_v<kWideThreads, 1, true>(arena_bytes, ctas_per_sm)
+                              : occupancy_v<kWideThreads, 1>(arena_bytes, ctas_per_sm);
+    case 5: return occupancy_v<kThreads, 5>(arena_bytes, ctas_per_sm);
+    case 6: return occupancy_v<kThreads, 6>(arena_bytes, ctas_per_sm);
+    default: return occupancy_v<kThreads, 4>(arena_bytes, ctas_per_sm);
   }
 }
 
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream) {
   switch (p.variant) {
-    case 5: return launch_v<5>(p, grid, stream);
-    case 6: return launch_v<6>(p, grid, stream);
-    default: return launch_v<4>(p, grid, stream);
+    case 1: return p.imf_off ? launch_v<kWideThreads, 1, true>(p, grid, stream)
+                             : launch_v<kWideThreads, 1>(p, grid, stream);
+    case 5: return launch_v<kThreads, 5>(p, grid, stream);
+    case 6: return launch_v<kThreads, 6>(p, grid, stream);
+    default: return launch_v<kThreads, 4>(p, grid, stream);
   }
 }
 

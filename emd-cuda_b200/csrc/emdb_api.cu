@@ -28,8 +28,8 @@ struct emdb_plan {
   int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
   unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes
   char* d_slab = nullptr;
-  size_t slab_stride = 0;
-  int slab_ctas = 0;
+  size_t slab_stride = 0;     // knot slab per CTA (the wide instance adds trace arrays)
+  size_t slab_bytes = 0;      // allocated
   // host-memory pipeline (emdb_run_host): device staging grown on demand, a
   // non-blocking copy stream, chunk counters and their mapped host flags
   char* d_stage = nullptr;
@@ -110,7 +110,7 @@ struct DeviceGuard {
 // traces, 223 vs 218 ms for 8,192).
 int auto_arena_for(int smem_optin, int variant, int nbsym, int max_n) {
   const int per_sm = 233472;
-  const size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1));
+  const size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1), variant);
   auto share = [&](int want) {
     int arena = std::min(per_sm / want - 1024, smem_optin);
     // shared memory is allocated in 128-byte units: a 16-byte-rounded share
@@ -138,17 +138,18 @@ int arena_for(const emdb_plan* p, int max_n) {
   return auto_arena(p, max_n);
 }
 
-int ensure_slab(emdb_plan* p, int grid) {
-  if (grid <= p->slab_ctas) return EMDB_OK;
+int ensure_slab(emdb_plan* p, size_t bytes) {
+  if (bytes <= p->slab_bytes) return EMDB_OK;
   if (p->d_slab) cudaFree(p->d_slab);
   p->d_slab = nullptr;
-  p->slab_ctas = 0;
-  size_t bytes = p->slab_stride * (size_t)grid;
+  p->slab_bytes = 0;
   cudaError_t e = cudaMalloc(&p->d_slab, bytes);
   if (e != cudaSuccess) return cuda_fail(e, "allocating the spill slab");
-  p->slab_ctas = grid;
+  p->slab_bytes = bytes;
   return EMDB_OK;
 }
+
+inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
 int check_config(const emdb_config* c) {
   if (!c) return fail(EMDB_ERR_INVALID, "config is NULL");
@@ -224,19 +225,44 @@ class ZeroRows {
 // Arena, occupancy and the launch-independent SiftParams fields; *grid = the
 // persistent grid for sp.batch traces.
 int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
+  int variant = p->variant;
   int arena = arena_for(p, max_n);
-  if (arena <= 0 || emdb::sift_fixed_smem(max_n) + 64 > (size_t)arena)
-    return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
-                " does not fit this device's shared memory");
+  bool gimf = false;
+  if (arena <= 0 || emdb::sift_fixed_smem(max_n, variant) + 64 > (size_t)arena) {
+    // Too long for the plan's instance: the wide instance at the full arena
+    // (the reference keeps whole traces in global memory, kernels.py:869-878,
+    // so it has no length limit; neither does this fallback): the proto-IMF in
+    // shared memory while it fits, else in the CTA's global slab.
+    variant = 1;
+    arena = p->smem_optin & ~127;
+    gimf = emdb::sift_fixed_smem(max_n, 1) + 64 > (size_t)arena;
+    if (emdb::sift_fixed_smem(max_n, 1, gimf) + 64 > (size_t)arena)
+      return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
+                  " does not fit this device's shared memory");
+  }
   int per_sm = 0;
-  cudaError_t e = emdb::sift_occupancy(arena, p->variant, &per_sm);
+  cudaError_t e = emdb::sift_occupancy(arena, variant, &per_sm, gimf);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
   *grid = std::min(sp.batch, per_sm * p->num_sms);
-  sp.variant = p->variant;
+  sp.variant = variant;
   sp.status = p->d_ctl + 1;
   sp.counters = p->d_cnt;
   sp.slab_stride = p->slab_stride;
+  sp.park_off = sp.q_off = sp.imf_off = 0;
+  if (emdb::variant_threads(variant) > emdb::kThreads) {
+    // the wide instance parks the proto-IMF and keeps the stop-test
+    // quotients in two trace-length arrays after the knot slab (and, for a
+    // trace longer than shared memory holds, the proto-IMF itself after them)
+    const size_t trace = al256((size_t)std::max(max_n, 1) * sizeof(double));
+    sp.park_off = al256(p->slab_stride);
+    sp.q_off = sp.park_off + trace;
+    sp.slab_stride = sp.q_off + trace;
+    if (gimf) {
+      sp.imf_off = sp.slab_stride;
+      sp.slab_stride += trace;
+    }
+  }
   sp.arena_bytes = arena;
   sp.max_extrema = p->cfg.max_extrema;
   sp.nbsym = p->cfg.nbsym;
@@ -249,7 +275,7 @@ int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st
   int grid = 0;
   int rc = prepare_sift(p, sp, max_n, &grid);
   if (rc) return rc;
-  rc = ensure_slab(p, grid);
+  rc = ensure_slab(p, sp.slab_stride * (size_t)grid);
   if (rc) return rc;
   sp.queue = p->d_ctl;
   sp.slab = p->d_slab;
@@ -345,7 +371,8 @@ int emdb_plan_set_arena(emdb_plan* p, int arena_bytes) {
 int emdb_plan_set_variant(emdb_plan* p, int min_ctas_per_sm) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (!emdb::sift_variant_ok(min_ctas_per_sm))
-    return fail(EMDB_ERR_INVALID, "variant must be 4, 5 or 6 CTAs per SM");
+    return fail(EMDB_ERR_INVALID,
+                "variant must be 4, 5 or 6 (128-thread CTAs) or 1 (512-thread wide CTAs)");
   std::lock_guard<std::mutex> lk(p->mu);
   p->variant = min_ctas_per_sm;
   return EMDB_OK;
@@ -510,7 +537,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     if (k == 0) base = sp;                     // arena and config fields are shared
   }
   size_t slab_need = 0;
-  for (int k = 0; k < ngroup; ++k) slab_need += (size_t)grid[k] * p->slab_stride;
+  for (int k = 0; k < ngroup; ++k) slab_need += (size_t)grid[k] * base.slab_stride;
   if (slab_need > p->group_slab_bytes) {
     if (p->d_group_slab) cudaFree(p->d_group_slab);
     p->d_group_slab = nullptr;
@@ -558,7 +585,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     sp.chunk_count = p->d_chunk_count + gstart[k] / chunk;
     sp.chunk_rows = p->d_chunk_rows + gstart[k] / chunk;
     sp.chunk_flag = p->d_chunk_flag + gstart[k] / chunk;
-    slab_off += (size_t)grid[k] * p->slab_stride;
+    slab_off += (size_t)grid[k] * base.slab_stride;
     e = emdb::launch_sift(sp, grid[k], p->group_stream[k]);
     if (e == cudaSuccess) e = cudaEventRecord(p->ev_group[k], p->group_stream[k]);
     if (e != cudaSuccess) return drain(e, "sift launch");
@@ -762,7 +789,7 @@ int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batc
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
   int grid = std::min(batch, per_sm * p->num_sms);
-  int rc = ensure_slab(p, grid);
+  int rc = ensure_slab(p, p->slab_stride * (size_t)grid);
   if (rc) return rc;
   emdb::EnvParams ep{};
   ep.values = signals;

@@ -8,6 +8,9 @@ namespace emdb {
 
 constexpr int kThreads = 128;   // one CTA = 128 threads = the reference's 128 reduction lanes
 constexpr int kWarps = kThreads / 32;
+// the wide instance: one long trace per SM, 16 warps; its reductions keep the
+// 128 lanes above
+constexpr int kWideThreads = 512;
 constexpr int kMaxNbsym = 8;
 constexpr int kMaxImfsCap = 64;
 
@@ -42,6 +45,10 @@ struct SiftParams {
   unsigned long long* counters;  // [0] sift passes, [1] passes on the global slab (may be NULL)
   char* slab;                 // per-CTA global spill area
   size_t slab_stride;         // bytes per CTA
+  size_t park_off;            // wide instance: parked proto-IMF at slab + park_off (bytes)
+  size_t q_off;               // wide instance: stop-test quotients at slab + q_off
+  size_t imf_off;             // wide instance, traces longer than shared memory holds: the
+                              // proto-IMF at slab + imf_off (0 = in shared memory)
   int arena_bytes;            // dynamic shared memory per CTA
   // chunk completion for copying finished traces back early (NULL = off):
   // traces [c*chunk_traces, (c+1)*chunk_traces) form chunk c
@@ -55,7 +62,8 @@ struct SiftParams {
   int nbsym;
   int max_iteration;
   int max_imfs;
-  int variant;                // register-budget variant: min CTAs per SM (4, 5, 6)
+  int variant;                // 4, 5, 6: 128-thread CTAs, register budget for that many per
+                              // SM; 1: the 512-thread wide instance, one CTA per SM
 };
 
 struct EnvParams {
@@ -84,8 +92,12 @@ struct EnvParams {
   int nbsym;
 };
 
-// Shared-memory bytes a CTA needs beyond the knot arena for a trace of length N.
-size_t sift_fixed_smem(int N);
+// Shared-memory bytes a CTA of the given variant needs beyond the knot arena
+// for a trace of length N (imf_global: the wide instance with the proto-IMF in
+// the global slab).
+size_t sift_fixed_smem(int N, int variant = 4, bool imf_global = false);
+// Threads per CTA of a kernel variant.
+int variant_threads(int variant);
 // Worst-case global spill bytes per CTA for a given extrema cap / nbsym.
 size_t sift_slab_bytes(int max_extrema, int nbsym);
 // Knot placement a sift pass takes for a trace of N samples in a CTA arena of
@@ -97,7 +109,8 @@ int sift_pass_placement(int N, int arena_total, size_t slab_stride, int kc0, int
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream);
 cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream);
 bool sift_variant_ok(int variant);
-cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm);
+cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm,
+                           bool imf_global = false);
 cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm);
 cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
                              unsigned long long* mismatches, cudaStream_t stream);

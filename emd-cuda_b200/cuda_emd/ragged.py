@@ -30,16 +30,24 @@ from . import _native
 from .kernels import EMDKernelConfig
 
 TIER_EDGES = (1024, 2048, 4096, 8192, 16384, 32768)
+WIDE = 1                  # plan variant of the wide instance (one 512-thread CTA per SM)
+WIDE_FROM = 4096          # tiers at least this long also try the wide instance
 SMEM_PER_SM = 233472      # B200: 228 KB per SM
 CTA_RESERVED = 1024       # shared memory the runtime reserves per CTA
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "emd_b200_autotune.json")
 
 
 def tier_of(n: int) -> int:
+    """Length tier of a trace: the listed edges, then powers of two (traces
+    past what a CTA's shared memory holds run on the wide instance with the
+    proto-IMF in global memory)."""
     for e in TIER_EDGES:
         if n <= e:
             return e
-    raise ValueError(f"trace length {n} exceeds the largest tier {TIER_EDGES[-1]}")
+    e = TIER_EDGES[-1]
+    while e < n:
+        e *= 2
+    return e
 
 
 def candidates(plan: _native.Plan, max_n: int) -> list[tuple[int, int]]:
@@ -58,6 +66,10 @@ def candidates(plan: _native.Plan, max_n: int) -> list[tuple[int, int]]:
         a = min((SMEM_PER_SM // k - CTA_RESERVED) & ~127, 232448)
         if a >= floor:
             out.append((max(k, 4), a))
+    if max_n >= WIDE_FROM:
+        # one 512-thread CTA per SM on one trace, at the automatic (full) arena;
+        # for traces too long for shared memory the only candidate
+        out.append((WIDE, 0))
     return out
 
 
@@ -97,8 +109,9 @@ class RaggedRunner:
         import torch
         name = torch.cuda.get_device_name(self.device)
         c = self.cfg
-        # "t2": entries timed on throughput-sized samples (older ones are ignored)
-        return f"t2|{name}|{c.max_extrema},{c.nbsym},{c.max_iteration},{c.max_imfs}|{edge}"
+        # "t3": entries timed on throughput-sized samples with the wide instance
+        # among the candidates (older ones are ignored)
+        return f"t3|{name}|{c.max_extrema},{c.nbsym},{c.max_iteration},{c.max_imfs}|{edge}"
 
     def _load_cache(self) -> dict:
         if self.cache_path and os.path.isfile(self.cache_path):

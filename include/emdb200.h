@@ -66,9 +66,14 @@ int emdb_plan_destroy(emdb_plan* plan);
  * autotuner sets this; larger arenas spill fewer knots but fit fewer CTAs
  * per SM.  Fails if the arena cannot hold a trace of length max_n. */
 int emdb_plan_set_arena(emdb_plan* plan, int arena_bytes);
-/* Register-budget variant of the sift kernel: the kernel instance compiled
- * for at least `min_ctas_per_sm` (4, 5 or 6) resident 128-thread CTAs per SM;
- * the automatic arena then targets that many CTAs.  Chosen by the autotuner. */
+/* Kernel instance of the sift: 4, 5 or 6 = 128-thread CTAs compiled for at
+ * least that many resident per SM (register budget), the automatic arena
+ * then targets that many CTAs; 1 = the wide instance, one 512-thread CTA per
+ * SM working on one trace (long traces: 16 warps and the knots on-chip),
+ * same results bit for bit.  Chosen by the autotuner.  A launch whose traces
+ * do not fit the plan's instance runs on the wide instance at the full
+ * shared-memory arena, with the proto-IMF in global memory when shared
+ * memory cannot hold it, so any trace length runs. */
 int emdb_plan_set_variant(emdb_plan* plan, int min_ctas_per_sm);
 /* Arena and CTAs/SM the plan would use for traces up to max_n. */
 int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,

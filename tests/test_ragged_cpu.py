@@ -34,8 +34,9 @@ def test_tier_edges():
     assert R.tier_of(1) == 1024 and R.tier_of(1024) == 1024
     assert R.tier_of(1025) == 2048 and R.tier_of(8192) == 8192
     assert R.tier_of(8193) == 16384
-    with pytest.raises(ValueError):
-        R.tier_of(R.TIER_EDGES[-1] + 1)
+    # past the listed edges: powers of two (the long-trace instance runs them)
+    assert R.tier_of(R.TIER_EDGES[-1] + 1) == 65536
+    assert R.tier_of(65537) == 131072 and R.tier_of(1 << 20) == 1 << 20
 
 
 @pytest.mark.parametrize("n", [256, 2048, 4096, 8192, 16384, 32768])
@@ -44,9 +45,16 @@ def test_candidates(n):
     cands = R.candidates(p, n)
     floor = p.min_arena(n)
     assert p.variant == 4 and p.arena == 0          # reset before the floor query
+    # the wide instance (one 512-thread CTA per SM, automatic arena) is offered
+    # for long tiers, last
+    wide = [c for c in cands if c[0] == R.WIDE]
+    assert wide == ([(R.WIDE, 0)] if n >= R.WIDE_FROM else [])
+    if wide:
+        assert cands[-1] == (R.WIDE, 0)
+    cands = [c for c in cands if c[0] != R.WIDE]
     if floor > 232448:
         # the proto-IMF alone exceeds a block's shared memory (N = 32768:
-        # 256 KB): no candidate, and the runner reports the tier as not fitting
+        # 256 KB): only the wide instance, which keeps it in global memory
         assert cands == [], n
         return
     assert cands, n
