@@ -48,14 +48,126 @@ class Request:
     done: float = 0.0
     delivered: float = 0.0
     result: tuple | None = None       # (imfs list of [n_imfs, N] arrays, n_imfs, overflow)
+    deadline: float | None = None     # server clock; past it the request is dropped as timed out
+    status: str = "new"               # pending, running, delivered, cancelled, timeout
 
     @property
     def nbytes(self) -> int:
         return int(sum(t.shape[0] for t in self.traces)) * 8
 
     @property
+    def max_len(self) -> int:
+        return max((int(t.shape[0]) for t in self.traces), default=0)
+
+    @property
     def latency(self) -> float:
         return self.delivered - self.arrival
+
+
+def cost_bytes(n_samples: int, n_traces: int, max_imfs: int) -> int:
+    """Device memory one launch holds: input + dense CSR output + per-trace
+    counts (and the offsets / order)."""
+    return n_samples * 8 * (1 + max_imfs) + n_traces * (4 * 3 * max_imfs + 24)
+
+
+class Admission:
+    """Which pending requests start next -- host logic only, no GPU.
+
+    Requests wait in one FIFO queue per lane: "short" (every trace at most
+    `short_max` samples) and "long".  Each lane has its own launch slots, so
+    requests whose sift runs for seconds (long traces past max_extrema run to
+    the iteration cap) never hold the slots short requests need.  All lanes
+    share one device-memory budget.  A batch takes requests from the head of
+    its lane's queue while they fit the budget and `max_batch` traces; a
+    request larger than the whole budget is admitted alone once nothing else
+    is in flight.  cancel() and expire() drop waiting requests (cancelled /
+    past their deadline) before they reach the device."""
+
+    LANES = ("short", "long")
+
+    def __init__(self, short_slots: int, long_slots: int, budget: int, max_batch: int,
+                 short_max: int, max_imfs: int):
+        self.max_batch = int(max_batch)
+        self.budget = int(budget)
+        self.short_max = int(short_max)
+        self.max_imfs = int(max_imfs)
+        self.queues = {lane: collections.deque() for lane in self.LANES}
+        # slot ids: short lane first
+        self.free = {"short": collections.deque(range(short_slots)),
+                     "long": collections.deque(range(short_slots, short_slots + long_slots))}
+        self.in_use = 0
+        self.running = 0                  # batches in flight
+        self.n_short = int(short_slots)
+
+    @property
+    def nslots(self) -> int:
+        return sum(len(q) for q in self.free.values()) + self.running
+
+    def lane_of(self, req: Request) -> str:
+        if not self.n_short:
+            return "long"                 # no short lane: one queue for everything
+        return "short" if req.max_len <= self.short_max else "long"
+
+    def submit(self, req: Request) -> None:
+        req.status = "pending"
+        self.queues[self.lane_of(req)].append(req)
+
+    def pending(self) -> int:
+        return sum(len(q) for q in self.queues.values())
+
+    def cancel(self, rid: int) -> Request | None:
+        """Drop a waiting request; None if it is not waiting (running or done)."""
+        for q in self.queues.values():
+            for r in q:
+                if r.rid == rid:
+                    q.remove(r)
+                    r.status = "cancelled"
+                    return r
+        return None
+
+    def expire(self, now: float) -> list:
+        """Drop the waiting requests whose deadline has passed."""
+        out = []
+        for q in self.queues.values():
+            for r in [r for r in q if r.deadline is not None and now > r.deadline]:
+                q.remove(r)
+                r.status = "timeout"
+                out.append(r)
+        return out
+
+    def next_batches(self, any_in_flight: bool) -> list:
+        """(slot, lane, requests, bytes) for every batch that can start now;
+        takes the slots and the budget."""
+        out = []
+        for lane in self.LANES:
+            q, free = self.queues[lane], self.free[lane]
+            while q and free:
+                batch, ntr, nsamp = [], 0, 0
+                while q:
+                    r = q[0]
+                    rs = sum(int(t.shape[0]) for t in r.traces)
+                    cost = cost_bytes(nsamp + rs, ntr + len(r.traces), self.max_imfs)
+                    if batch and (ntr + len(r.traces) > self.max_batch or self.in_use + cost > self.budget):
+                        break
+                    if not batch and self.in_use + cost > self.budget and (any_in_flight or out):
+                        break                   # wait for memory to free up
+                    batch.append(q.popleft())
+                    ntr += len(r.traces)
+                    nsamp += rs
+                if not batch:
+                    break
+                b = cost_bytes(nsamp, ntr, self.max_imfs)
+                self.in_use += b
+                self.running += 1
+                for r in batch:
+                    r.status = "running"
+                out.append((free.popleft(), lane, batch, b))
+        return out
+
+    def release(self, slot: int, lane: str, nbytes: int) -> None:
+        self.in_use -= nbytes
+        self.running -= 1
+        self.free[lane].append(slot)
 
 
 @dataclass
@@ -68,15 +180,22 @@ class _Flight:
     offsets_h: np.ndarray
     budget: int
     first: list                       # first trace index of each request
-    state: list                       # per request: 0 running, 1 copying, 2 delivered
+    state: list                       # per request: 0 running, 1 copying, 2 delivered, 3 dropped
     copies: list                      # per request: event of its copy-back
     keep: tuple = field(default_factory=tuple)
+    lane: str = "long"
+    start: object = None              # timing event before the launch's kernels
 
 
 class EMDServer:
+    """Continuous-batching server.  `slots` launch slots serve requests with a
+    trace longer than `short_max` samples, `short_slots` more serve the
+    others (Admission)."""
+
     def __init__(self, config: EMDKernelConfig | None = None, device: int | None = None,
                  slots: int = 4, hbm_budget_bytes: int = 32 << 30, max_batch_traces: int = 4096,
-                 cost_model=None, adaptive_arena: bool = True):
+                 cost_model=None, adaptive_arena: bool = True, short_slots: int = 2,
+                 short_max: int = 4096):
         import torch
         self.cfg = config or EMDKernelConfig()
         self.device = torch.cuda.current_device() if device is None else int(device)
@@ -86,21 +205,25 @@ class EMDServer:
         self.smem_optin = props.shared_memory_per_block_optin
         self.adaptive_arena = adaptive_arena
         self.min_arena: dict[int, int] = {}
-        self.nslots = slots
+        self.nslots = slots + short_slots
         self.budget = int(hbm_budget_bytes)
         self.max_batch = max_batch_traces
         self.cost_model = cost_model
-        self.streams = [torch.cuda.Stream(self.device) for _ in range(slots)]
+        self.adm = Admission(short_slots, slots, hbm_budget_bytes, max_batch_traces, short_max,
+                             self.cfg.max_imfs)
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(self.nslots)]
         self.copy_stream = torch.cuda.Stream(self.device)
-        self.notify = [_native.Notify(max_batch_traces, self.device) for _ in range(slots)]
+        self.notify = [_native.Notify(max_batch_traces, self.device) for _ in range(self.nslots)]
         self.plans: dict[tuple[int, int], _native.Plan] = {}
         self.tier_streams: dict = {}
-        self.free_slots = collections.deque(range(slots))
-        self.pending: collections.deque[Request] = collections.deque()
         self.flights: list[_Flight] = []
-        self.in_use = 0
         self.t0 = time.perf_counter()
         self.completed: list[Request] = []
+        self.dropped: list[Request] = []
+        # device clock origin for the launches' start / end events
+        self.ev0 = torch.cuda.Event(enable_timing=True)
+        self.ev0.record(torch.cuda.current_stream(self.device))
+        self.intervals: list = []         # (lane, start event, end event) per launch
 
     def now(self) -> float:
         return time.perf_counter() - self.t0
@@ -109,12 +232,49 @@ class EMDServer:
     def submit(self, req: Request) -> None:
         if not req.arrival:
             req.arrival = self.now()
-        self.pending.append(req)
+        self.adm.submit(req)
 
-    @staticmethod
-    def _cost_bytes(n_samples: int, n_traces: int, max_imfs: int) -> int:
-        # input + dense CSR output + per-trace counts (and the offsets / order)
-        return n_samples * 8 * (1 + max_imfs) + n_traces * (4 * 3 * max_imfs + 24)
+    @property
+    def pending(self) -> int:
+        return self.adm.pending()
+
+    @property
+    def in_use(self) -> int:
+        return self.adm.in_use
+
+    def cancel(self, rid: int) -> bool:
+        """Cancel a request: a waiting one never reaches the device; a running
+        one keeps its launch going (the kernel is not interrupted) but is not
+        copied back or delivered.  False if it is unknown or already done."""
+        r = self.adm.cancel(rid)
+        if r is not None:
+            self.dropped.append(r)
+            return True
+        for f in self.flights:
+            for q, r in enumerate(f.reqs):
+                if r.rid == rid and f.state[q] in (0, 1):
+                    f.state[q] = 3
+                    r.status = "cancelled"
+                    self.dropped.append(r)
+                    return True
+        return False
+
+    def _expire(self) -> None:
+        now = self.now()
+        self.dropped.extend(self.adm.expire(now))
+        for f in self.flights:
+            for q, r in enumerate(f.reqs):
+                if f.state[q] == 0 and r.deadline is not None and now > r.deadline:
+                    f.state[q] = 3
+                    r.status = "timeout"
+                    self.dropped.append(r)
+
+    _cost_bytes = staticmethod(cost_bytes)
+
+    def device_intervals(self) -> list:
+        """(lane, start ms, end ms) on the device clock of every finished launch."""
+        return [(lane, self.ev0.elapsed_time(a), self.ev0.elapsed_time(b))
+                for lane, a, b in self.intervals if b.query()]
 
     def _tier_stream(self, slot: int, edge: int):
         import torch
@@ -151,38 +311,23 @@ class EMDServer:
         return arena if arena >= m else 0
 
     def _admit(self) -> int:
-        """Admit pending requests into free slots while the budget allows."""
-        import torch
+        """Admit pending requests into free slots of their lanes while the budget allows."""
         admitted = 0
-        while self.pending and self.free_slots:
-            batch, ntr, nsamp = [], 0, 0
-            while self.pending:
-                r = self.pending[0]
-                rs = sum(t.shape[0] for t in r.traces)
-                cost = self._cost_bytes(nsamp + rs, ntr + len(r.traces), self.cfg.max_imfs)
-                if batch and (ntr + len(r.traces) > self.max_batch or self.in_use + cost > self.budget):
-                    break
-                if not batch and self.in_use + cost > self.budget and self.flights:
-                    break                       # wait for memory to free up
-                batch.append(self.pending.popleft())
-                ntr += len(r.traces)
-                nsamp += rs
-            if not batch:
-                break
-            slot = self.free_slots.popleft()
-            self._launch(slot, batch, ntr, nsamp)
+        for slot, lane, batch, nbytes in self.adm.next_batches(bool(self.flights)):
+            ntr = sum(len(r.traces) for r in batch)
+            nsamp = sum(int(t.shape[0]) for r in batch for t in r.traces)
+            self._launch(slot, batch, ntr, nsamp, lane, nbytes)
             admitted += len(batch)
         return admitted
 
-    def _launch(self, slot: int, reqs: list, ntr: int, nsamp: int) -> None:
+    def _launch(self, slot: int, reqs: list, ntr: int, nsamp: int, lane: str = "long",
+                budget: int = 0) -> None:
         import torch
         st = self.streams[slot]
         lens = np.array([t.shape[0] for r in reqs for t in r.traces], dtype=np.int64)
         off_h = np.zeros(ntr + 1, dtype=np.int64)
         np.cumsum(lens, out=off_h[1:])
         vals_h = np.concatenate([t for r in reqs for t in r.traces]) if ntr else np.zeros(0)
-        budget = self._cost_bytes(nsamp, ntr, self.cfg.max_imfs)
-        self.in_use += budget
         now = self.now()
         for r in reqs:
             r.admitted = now
@@ -215,7 +360,7 @@ class EMDServer:
                     order = order[torch.argsort(sub, descending=True, stable=True)]
                 keep.append(order)
                 tiers.append((e, idx.size, order))
-            ready = torch.cuda.Event()
+            ready = torch.cuda.Event(enable_timing=True)
             ready.record(st)
         # each tier on its own stream of the slot, so a short tier's traces
         # (and the requests they finish) need not wait for a long tier
@@ -233,8 +378,9 @@ class EMDServer:
             done_t = torch.cuda.Event()
             done_t.record(ts)
             st.wait_event(done_t)
-        ev = torch.cuda.Event()
+        ev = torch.cuda.Event(enable_timing=True)
         ev.record(st)
+        self.intervals.append((lane, ready, ev))
         h_imfs = torch.empty(mi * nsamp, dtype=torch.float64).pin_memory()
         h_n = torch.empty(ntr, dtype=torch.int32).pin_memory()
         h_o = torch.empty(ntr, dtype=torch.int32).pin_memory()
@@ -245,7 +391,8 @@ class EMDServer:
         first.append(k)
         keep.extend([dn, de, dz])
         self.flights.append(_Flight(slot, reqs, ev, (h_imfs, h_n, h_o), (imfs, n_imfs, ovf), off_h,
-                                    budget, first, [0] * len(reqs), [None] * len(reqs), tuple(keep)))
+                                    budget, first, [0] * len(reqs), [None] * len(reqs), tuple(keep),
+                                    lane, ready))
 
     # -- completion -------------------------------------------------------------
     def _copy_request(self, f: _Flight, q: int, flags: np.ndarray) -> None:
@@ -284,6 +431,7 @@ class EMDServer:
         r.done = self.now()
         r.result = (rows, np.array(nims, dtype=np.int32), np.array(ovfs, dtype=np.int32))
         r.delivered = self.now()
+        r.status = "delivered"
         self.completed.append(r)
         f.state[q] = 2
 
@@ -303,9 +451,8 @@ class EMDServer:
                 if f.state[q] == 1 and f.copies[q].query():
                     self._deliver(f, q)
                     done += 1
-            if kernels_done and all(st == 2 for st in f.state):
-                self.in_use -= f.budget
-                self.free_slots.append(f.slot)
+            if kernels_done and all(st in (2, 3) for st in f.state):
+                self.adm.release(f.slot, f.lane, f.budget)
             else:
                 still.append(f)
         self.flights = still
@@ -315,6 +462,7 @@ class EMDServer:
         """One scheduler tick: reap finished launches, admit pending requests."""
         import torch
         with torch.cuda.nvtx.range("serve reap"):
+            self._expire()
             d = self._reap()
         with torch.cuda.nvtx.range("serve admit"):
             a = self._admit()

@@ -48,13 +48,13 @@ def test_server_alone_equals_in_mix():
     # each request alone
     alone = []
     for r in reqs:
-        srv = EMDServer(slots=1)
+        srv = EMDServer(slots=1, short_slots=0)
         rr = Request(r.rid, r.traces)
         srv.submit(rr)
         srv.drain(timeout_s=120)
         alone.append(rr.result)
     # all of them in one open-loop run with overlapping arrivals
-    srv = EMDServer(slots=3, max_batch_traces=48)
+    srv = EMDServer(slots=3, max_batch_traces=16)
     mix = [Request(r.rid, r.traces) for r in reqs]
     arr = np.cumsum(np.full(len(mix), 0.002))
     rep = run_open_loop(srv, mix, arr, timeout_s=300)
@@ -67,8 +67,11 @@ def test_server_alone_equals_in_mix():
         np.testing.assert_array_equal(o_a, o_m)
         for x, y in zip(rows_a, rows_m):
             np.testing.assert_array_equal(x, y)
-    # several admissions actually overlapped on the device
-    assert max(r.admitted for r in mix) < max(r.done for r in mix)
+    # two launches ran on the device at the same time: their start / end
+    # events (device clock) overlap
+    iv = srv.device_intervals()
+    assert len(iv) >= 2
+    assert any(a[1] < b[2] and b[1] < a[2] for i, a in enumerate(iv) for b in iv[i + 1:]), iv
 
 
 def test_server_hbm_budget_limits_admission():
@@ -95,11 +98,11 @@ def test_short_request_is_not_held_by_a_long_one():
     from cuda_emd.serving import EMDServer, Request
     rng = np.random.default_rng(8)
     long_tr, short_tr = W.chirp_trace(rng, 8192), W.sinusoid_trace(rng, 256)
-    alone = EMDServer(slots=1)
+    alone = EMDServer(slots=1, short_slots=0)
     solo = Request(9, [short_tr])
     alone.submit(solo)
     alone.drain(timeout_s=120)
-    srv = EMDServer(slots=1)
+    srv = EMDServer(slots=1, short_slots=0)       # one lane: both in one launch
     a, b = Request(0, [long_tr]), Request(1, [short_tr])
     srv.submit(a)
     srv.submit(b)
@@ -112,3 +115,51 @@ def test_short_request_is_not_held_by_a_long_one():
     for x, y in zip(solo.result[0], b.result[0]):
         np.testing.assert_array_equal(x, y)
     np.testing.assert_array_equal(solo.result[1], b.result[1])
+
+
+def test_short_lane_is_not_blocked_by_long_requests():
+    """Length lanes: a short request arriving while long requests hold every
+    long-lane slot is admitted at once into the short lane and delivered long
+    before them, with the same results as alone."""
+    from cuda_emd import workloads as W
+    from cuda_emd.serving import EMDServer, Request
+    rng = np.random.default_rng(9)
+    longs = [Request(i, [W.chirp_trace(rng, 8192)]) for i in range(3)]
+    short = Request(10, [W.sinusoid_trace(rng, 512)])
+    srv = EMDServer(slots=2, short_slots=1, max_batch_traces=1)
+    for r in longs:
+        srv.submit(r)
+    srv.step()                                       # two long launches, one waiting
+    srv.submit(short)
+    srv.drain(timeout_s=120)
+    assert short.admitted <= min(r.done for r in longs)
+    assert short.delivered < min(r.delivered for r in longs)
+    solo = EMDServer(slots=1, short_slots=0)
+    s2 = Request(11, short.traces)
+    solo.submit(s2)
+    solo.drain(timeout_s=60)
+    for x, y in zip(s2.result[0], short.result[0]):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_cancel_and_deadline_on_the_device():
+    """A request cancelled while running and one whose deadline passes while
+    waiting are not delivered; the others are, unchanged, and every slot
+    and byte of budget is released."""
+    from cuda_emd.serving import EMDServer, Request, make_requests
+    rng = np.random.default_rng(12)
+    reqs = make_requests(6, rng, lo=512, hi=2048, max_traces=4)
+    srv = EMDServer(slots=1, short_slots=1, max_batch_traces=4)
+    for r in reqs:
+        srv.submit(r)
+    srv.step()
+    running = [r for r in reqs if r.status == "running"]
+    assert running and srv.cancel(running[0].rid)
+    waiting = [r for r in reqs if r.status == "pending"]
+    waiting[-1].deadline = srv.now() - 1.0           # already past
+    srv.drain(timeout_s=120)
+    assert running[0].status == "cancelled" and running[0].result is None
+    assert waiting[-1].status == "timeout" and waiting[-1].result is None
+    rest = [r for r in reqs if r not in (running[0], waiting[-1])]
+    assert all(r.status == "delivered" and r.result is not None for r in rest)
+    assert srv.in_use == 0 and srv.adm.nslots == 2 and srv.adm.running == 0

@@ -53,3 +53,69 @@ def test_cost_bytes_counts_inputs_outputs_and_counts():
     mi = 16
     b = serving.EMDServer._cost_bytes(1000, 3, mi)
     assert b == 1000 * 8 * (1 + mi) + 3 * (4 * 3 * mi + 24)
+
+
+# -- admission policy (lanes, budget, cancel, deadlines): host logic only --------
+
+def _req(rid, lens):
+    import numpy as np
+    return serving.Request(rid, [np.zeros(n) for n in lens])
+
+
+def _adm(short=1, long=2, budget=1 << 40, max_batch=64):
+    return serving.Admission(short, long, budget, max_batch, short_max=4096, max_imfs=16)
+
+
+def test_lanes_route_by_longest_trace():
+    a = _adm()
+    assert a.lane_of(_req(0, [100, 4096])) == "short"
+    assert a.lane_of(_req(1, [100, 4097])) == "long"
+    assert _adm(short=0).lane_of(_req(2, [100])) == "long"      # no short lane: one queue
+
+
+def test_short_requests_pass_long_ones_that_hold_every_long_slot():
+    a = _adm(short=1, long=1, max_batch=1)
+    for i in range(3):
+        a.submit(_req(i, [8192]))
+    first = a.next_batches(False)
+    assert [(lane, [r.rid for r in b]) for _, lane, b, _ in first] == [("long", [0])]
+    a.submit(_req(9, [512]))                       # long lane full, two long ones waiting
+    nxt = a.next_batches(True)
+    assert [(lane, [r.rid for r in b]) for _, lane, b, _ in nxt] == [("short", [9])]
+    assert a.pending() == 2
+
+
+def test_budget_batches_and_release():
+    one = serving.cost_bytes(1000, 1, 16)
+    a = _adm(short=2, long=0, budget=2 * one)
+    for i in range(4):
+        a.submit(_req(i, [1000]))
+    b = a.next_batches(False)
+    assert len(b) == 1 and [r.rid for r in b[0][2]] == [0, 1]    # two fit the budget together
+    assert a.next_batches(True) == []                            # the budget is spent
+    slot, lane, reqs, nbytes = b[0]
+    assert nbytes == serving.cost_bytes(2000, 2, 16) and a.in_use == nbytes
+    a.release(slot, lane, nbytes)
+    assert a.in_use == 0 and [r.rid for r in a.next_batches(False)[0][2]] == [2, 3]
+
+
+def test_oversized_request_runs_alone_when_the_device_is_idle():
+    a = _adm(short=2, long=0, budget=10)
+    a.submit(_req(0, [1000]))
+    assert a.next_batches(True) == []              # something in flight: wait
+    b = a.next_batches(False)
+    assert len(b) == 1 and b[0][2][0].rid == 0
+
+
+def test_cancel_and_expire_waiting_requests():
+    a = _adm(short=1, long=1)
+    r0, r1, r2 = _req(0, [100]), _req(1, [9000]), _req(2, [100])
+    r2.deadline = 5.0
+    for r in (r0, r1, r2):
+        a.submit(r)
+    assert a.cancel(1) is r1 and r1.status == "cancelled"
+    assert a.cancel(1) is None                     # not waiting any more
+    assert a.expire(4.0) == []
+    assert a.expire(6.0) == [r2] and r2.status == "timeout"
+    b = a.next_batches(False)
+    assert [r.rid for _, _, rs, _ in b for r in rs] == [0] and r0.status == "running"
