@@ -224,7 +224,14 @@ class ZeroRows {
 
 // Arena, occupancy and the launch-independent SiftParams fields; *grid = the
 // persistent grid for sp.batch traces.
+// Longest trace a launch takes: the per-warp extrema prefixes of the scan
+// masks are 16-bit, so at most 2^17 samples (< 2^16 extrema of a kind).
+constexpr int kMaxTraceLen = 1 << 17;
+
 int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
+  if (max_n > kMaxTraceLen)
+    return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
+                " exceeds the longest supported trace (131072 samples)");
   int variant = p->variant;
   int arena = arena_for(p, max_n);
   bool gimf = false;
