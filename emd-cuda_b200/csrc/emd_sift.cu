@@ -1884,7 +1884,9 @@ cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
 }
 
 size_t sift_fixed_smem(int N, int variant, bool imf_global) {
-  if (variant_threads(variant) <= kThreads) return fixed_bytes(N) + kRedBytes;
+  const int nt = variant_threads(variant);
+  if (nt <= kThreads) return fixed_bytes(N) + kRedBytes;
+  if (nt == kHalfWideThreads) return fixed_bytes<kHalfWideThreads>(N) + kRedBytes;
   return (imf_global ? fixed_bytes<kWideThreads, true>(N) : fixed_bytes<kWideThreads>(N)) +
          kRedBytes;
 }
@@ -1938,14 +1940,17 @@ cudaError_t launch_v(const SiftParams& p, int grid, cudaStream_t stream) {
 }
 }  // namespace
 
-bool sift_variant_ok(int v) { return v == 1 || v == 4 || v == 5 || v == 6; }
+bool sift_variant_ok(int v) { return v == 1 || v == 2 || v == 4 || v == 5 || v == 6; }
 
-int variant_threads(int v) { return v == 1 ? kWideThreads : kThreads; }
+int variant_threads(int v) {
+  return v == 1 ? kWideThreads : v == 2 ? kHalfWideThreads : kThreads;
+}
 
 cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm, bool imf_global) {
   switch (variant) {
     case 1: return imf_global ? occupancy_v<kWideThreads, 1, true>(arena_bytes, ctas_per_sm)
                               : occupancy_v<kWideThreads, 1>(arena_bytes, ctas_per_sm);
+    case 2: return occupancy_v<kHalfWideThreads, 2>(arena_bytes, ctas_per_sm);
     case 5: return occupancy_v<kThreads, 5>(arena_bytes, ctas_per_sm);
     case 6: return occupancy_v<kThreads, 6>(arena_bytes, ctas_per_sm);
     default: return occupancy_v<kThreads, 4>(arena_bytes, ctas_per_sm);
@@ -1956,6 +1961,7 @@ cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream) {
   switch (p.variant) {
     case 1: return p.imf_off ? launch_v<kWideThreads, 1, true>(p, grid, stream)
                              : launch_v<kWideThreads, 1>(p, grid, stream);
+    case 2: return launch_v<kHalfWideThreads, 2>(p, grid, stream);
     case 5: return launch_v<kThreads, 5>(p, grid, stream);
     case 6: return launch_v<kThreads, 6>(p, grid, stream);
     default: return launch_v<kThreads, 4>(p, grid, stream);

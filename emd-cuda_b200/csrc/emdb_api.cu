@@ -379,7 +379,8 @@ int emdb_plan_set_variant(emdb_plan* p, int min_ctas_per_sm) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (!emdb::sift_variant_ok(min_ctas_per_sm))
     return fail(EMDB_ERR_INVALID,
-                "variant must be 4, 5 or 6 (128-thread CTAs) or 1 (512-thread wide CTAs)");
+                "variant must be 4, 5 or 6 (128-thread CTAs), 2 (256-thread CTAs) or 1 "
+                "(512-thread wide CTAs)");
   std::lock_guard<std::mutex> lk(p->mu);
   p->variant = min_ctas_per_sm;
   return EMDB_OK;

@@ -11,6 +11,8 @@ constexpr int kWarps = kThreads / 32;
 // the wide instance: one long trace per SM, 16 warps; its reductions keep the
 // 128 lanes above
 constexpr int kWideThreads = 512;
+// half-wide: two 256-thread CTAs per SM, each on one trace
+constexpr int kHalfWideThreads = 256;
 constexpr int kMaxNbsym = 8;
 constexpr int kMaxImfsCap = 64;
 
@@ -63,7 +65,8 @@ struct SiftParams {
   int max_iteration;
   int max_imfs;
   int variant;                // 4, 5, 6: 128-thread CTAs, register budget for that many per
-                              // SM; 1: the 512-thread wide instance, one CTA per SM
+                              // SM; 1: the 512-thread wide instance, one CTA per SM;
+                              // 2: 256-thread CTAs, two per SM
 };
 
 struct EnvParams {

@@ -31,7 +31,9 @@ from .kernels import EMDKernelConfig
 
 TIER_EDGES = (1024, 2048, 4096, 8192, 16384, 32768)
 WIDE = 1                  # plan variant of the wide instance (one 512-thread CTA per SM)
+HALF_WIDE = 2             # plan variant of two 256-thread CTAs per SM
 WIDE_FROM = 4096          # tiers at least this long also try the wide instance
+HALF_WIDE_FROM = 2048     # ... and this long the half-wide one
 SMEM_PER_SM = 233472      # B200: 228 KB per SM
 CTA_RESERVED = 1024       # shared memory the runtime reserves per CTA
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "emd_b200_autotune.json")
@@ -66,6 +68,9 @@ def candidates(plan: _native.Plan, max_n: int) -> list[tuple[int, int]]:
         a = min((SMEM_PER_SM // k - CTA_RESERVED) & ~127, 232448)
         if a >= floor:
             out.append((max(k, 4), a))
+    if max_n >= HALF_WIDE_FROM and min((SMEM_PER_SM // 2 - CTA_RESERVED) & ~127, 232448) >= floor + 1024:
+        # two 256-thread CTAs per SM, at the automatic (half-SM) arena
+        out.append((HALF_WIDE, 0))
     if max_n >= WIDE_FROM:
         # one 512-thread CTA per SM on one trace, at the automatic (full) arena;
         # for traces too long for shared memory the only candidate

@@ -1,5 +1,6 @@
-"""GPU parity of the wide sift instance (plan variant 1: one 512-thread CTA per
-SM on one trace) and of its long-trace form (proto-IMF in global memory).
+"""GPU parity of the wide sift instances (plan variant 1: one 512-thread CTA
+per SM on one trace; variant 2: two 256-thread CTAs per SM) and of the
+long-trace form (proto-IMF in global memory).
 It must give the same bits as the 128-thread instance and the oracle on every
 path: the golden groups (both time-axis builds), long traces past
 max_extrema with every knot placement forced by the arena size, ragged CSR
@@ -39,15 +40,16 @@ def _run(L, X, T=None):
     return [o.cpu().numpy() for o in out]
 
 
+@pytest.mark.parametrize("variant", [1, 2])
 @pytest.mark.parametrize("name", [g["name"] for g in cases.groups()])
-def test_wide_golden_bitexact(golden, name):
+def test_wide_golden_bitexact(golden, name, variant):
     from cuda_emd import EMDKernelConfig
     X = golden[f"{name}__signals"]
     T = golden[f"{name}__T"]
     c = golden[f"{name}__cfg"]
     cfg = EMDKernelConfig(max_extrema=int(c[0]), nbsym=int(c[1]), max_iteration=int(c[2]),
                           max_imfs=int(c[3]))
-    L = _launcher(cfg)
+    L = _launcher(cfg, variant=variant)
     axes = [T]
     if np.array_equal(T, np.arange(X.shape[1], dtype=np.float64)):
         axes.append(None)                      # the integer-axis build too
@@ -81,6 +83,10 @@ def test_wide_equals_narrow_on_long_overflowing_traces(N):
         out = _run(_launcher(cfg, arena=arena), X)
         for a, b in zip(ref, out):
             assert np.array_equal(a, b), (N, arena)
+    # two 256-thread CTAs per SM, automatic (half-SM) arena
+    out = _run(_launcher(cfg, variant=2), X)
+    for a, b in zip(ref, out):
+        assert np.array_equal(a, b), (N, "half-wide")
 
 
 def test_wide_ragged_per_trace_time_axis_matches_oracle():

@@ -51,7 +51,11 @@ def test_candidates(n):
     assert wide == ([(R.WIDE, 0)] if n >= R.WIDE_FROM else [])
     if wide:
         assert cands[-1] == (R.WIDE, 0)
-    cands = [c for c in cands if c[0] != R.WIDE]
+    # and two 256-thread CTAs per SM for tiers from 2048 samples that fit half an SM
+    half = [c for c in cands if c[0] == R.HALF_WIDE]
+    fits_half = (233472 // 2 - 1024) & ~127 >= floor + 1024
+    assert half == ([(R.HALF_WIDE, 0)] if n >= R.HALF_WIDE_FROM and fits_half else [])
+    cands = [c for c in cands if c[0] not in (R.WIDE, R.HALF_WIDE)]
     if floor > 232448:
         # the proto-IMF alone exceeds a block's shared memory (N = 32768:
         # 256 KB): only the wide instance, which keeps it in global memory
