@@ -242,6 +242,12 @@ def main():
     ap.add_argument("--train-traces", type=int, default=200000, help="ragged64k: MLP training set")
     ap.add_argument("--eval-traces", type=int, default=0, help="ragged64k: batch size (0 = 65536)")
     ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--no-split", action="store_true",
+                    help="ragged64k: the model only orders queues, tiers stay by length")
+    ap.add_argument("--heavy-passes", type=float, default=600.0,
+                    help="ragged64k: predicted sift passes from which a trace goes wide")
+    ap.add_argument("--heavy-boost", type=float, default=1.0,
+                    help="ragged64k: wide launches' SM share = predicted work share x this")
     ap.add_argument("--requests", type=int, default=160, help="serve: requests per load level")
     ap.add_argument("--loads", default="0.1,0.3,0.5,0.7,0.9,1.1", help="serve: offered loads")
     ap.add_argument("--serve-requests", type=int, default=160,
@@ -737,7 +743,7 @@ def run_ragged(a, rank, world, pool, cores):
     o = torch.from_numpy(ev_offs).to(dev)
     lens_h = np.diff(ev_offs)
     B = n_eval
-    runner = RaggedRunner(cfg, device=local)
+    runner = RaggedRunner(cfg, device=local, heavy_passes=a.heavy_passes, heavy_boost=a.heavy_boost)
     st = torch.cuda.current_stream(dev)
 
     def timed(arm, steps, warm, clocks=None):
@@ -801,16 +807,21 @@ def run_ragged(a, rank, world, pool, cores):
     torch.cuda.empty_cache()
 
     # learned: features + BF16 inference + per-tier order + the launches, every step
-    lens_d = o[1:] - o[:-1]
 
-    def learned(outs, mark=None):
-        feats = S.features(v, o)
-        cost = S.predicted_cost(cm, feats, lens_d)
-        tiers_, orders_ = runner.prepare(v, o, cost, offsets_host=ev_offs)   # device-side order
+    def learned(outs, mark=None, split=not a.no_split):
+        # features + BF16 inference on the device; the model orders each
+        # tier's queue and (split) sends predicted-heavy traces to the wide
+        # instance, which needs the per-trace prediction on the host
+        tiers_, orders_ = runner.prepare_learned(v, o, cm, offsets_host=ev_offs, split_heavy=split)
         if mark is not None:
             mark.record(st)
         return runner.launch(tiers_, orders_, v, o, outs, use_graph=True)
 
+    def learned_order_only(outs, mark=None):
+        return learned(outs, mark, split=False)
+
+    k_side = min(a.steps, 5)
+    _, order_s, _ = timed(learned_order_only, k_side, 1)
     learned_out, learned_s, learned_launch = timed(learned, a.steps, a.warmup, clk)
     same = all(torch.equal(x, y) for x, y in zip(plain_copy, learned_out))
     # ceiling: the queue ordered by the TRUE cost (N x logged passes, known only afterwards)
@@ -823,7 +834,7 @@ def run_ragged(a, rank, world, pool, cores):
             mark.record(st)
         return runner.launch(tiers_, orders_, v, o, outs, use_graph=True)
 
-    k_true = min(a.steps, 5)
+    k_true = k_side
     _, true_s, _ = timed(oracle_order, k_true, 1)
     feats = S.features(v, o)
     truth = S.labels_from_debug(plain_copy[3], plain_copy[1])
@@ -838,9 +849,9 @@ def run_ragged(a, rank, world, pool, cores):
     tiers = {}
     for t in runner._tiers.values():
         t.plan.counters(reset=True)
-    runner.run_learned(v, o, cm, use_graph=False, offsets_host=ev_offs)
+    runner.run_learned(v, o, cm, use_graph=False, offsets_host=ev_offs, split_heavy=not a.no_split)
     torch.cuda.synchronize(dev)
-    for t in runner._tiers.values():
+    for t in runner._prep[1]:
         ps, sp = t.plan.counters(reset=True)
         sub = torch.from_numpy(t.idx.astype(np.int32)).to(dev)
         outs = runner._alloc_out(v, o)
@@ -849,7 +860,8 @@ def run_ragged(a, rank, world, pool, cores):
         runner._launch_tier(t, v, o, sub, outs)
         e1.record()
         e1.synchronize()
-        tiers[str(t.edge)] = {"traces": int(t.idx.size), "arena": t.arena, "variant": t.variant,
+        name = str(t.edge) + ("-heavy" if t in runner._heavy_tiers.values() else "")
+        tiers[name] = {"traces": int(t.idx.size), "arena": t.arena, "variant": t.variant,
                               "passes": ps, "spilled_frac": round(sp / max(ps, 1), 4),
                               "alone_ms": round(e0.elapsed_time(e1), 2)}
         del outs
@@ -860,14 +872,14 @@ def run_ragged(a, rank, world, pool, cores):
         vals_pin = torch.from_numpy(ev_vals).pin_memory()
         offs_pin = torch.from_numpy(ev_offs).pin_memory()
         for _ in range(max(1, min(a.warmup, 2))):
-            runner.run_host(vals_pin, offs_pin, model=cm)
+            runner.run_host(vals_pin, offs_pin, model=cm, split_heavy=not a.no_split)
         torch.cuda.synchronize(dev)
         R.barrier(world)
         t_0 = time.perf_counter()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
         for _ in range(a.steps):
-            res = runner.run_host(vals_pin, offs_pin, model=cm)
+            res = runner.run_host(vals_pin, offs_pin, model=cm, split_heavy=not a.no_split)
         e1.record(st)
         torch.cuda.synchronize(dev)
         wall = time.perf_counter() - t_0
@@ -937,6 +949,12 @@ def run_ragged(a, rank, world, pool, cores):
                         "launch_ms": round(learned_launch * 1e3, 3),
                         "speedup_vs_plain": round(plain_s / learned_s, 4),
                         "bit_identical_to_fifo": bool(same),
+                        "tier_choice": ("predicted-heavy traces (>= %g passes) of tiers >= %d "
+                                        "samples on the wide instance" % (runner.heavy_passes,
+                                                                          4096))
+                                       if not a.no_split else "by length only",
+                        "order_only_ms_per_step": round(order_s * 1e3, 3),
+                        "speedup_order_only": round(plain_s / order_s, 4),
                         "speedup_true_cost": round(plain_s / true_s, 4),
                         "true_cost_ms_per_step": round(true_s * 1e3, 3),
                         "true_cost_note": "queue ordered by N x the trace's logged sift passes "

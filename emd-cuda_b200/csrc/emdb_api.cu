@@ -25,6 +25,7 @@ struct emdb_plan {
   int smem_optin = 0;
   int arena_override = 0;
   int variant = 4;            // register-budget variant (min CTAs per SM)
+  int max_ctas = 0;           // cap on a launch's persistent grid (0 = resident CTAs)
   int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
   unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes
   char* d_slab = nullptr;
@@ -252,6 +253,7 @@ int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
   *grid = std::min(sp.batch, per_sm * p->num_sms);
+  if (p->max_ctas > 0) *grid = std::min(*grid, p->max_ctas);
   sp.variant = variant;
   sp.status = p->d_ctl + 1;
   sp.counters = p->d_cnt;
@@ -383,6 +385,14 @@ int emdb_plan_set_variant(emdb_plan* p, int min_ctas_per_sm) {
                 "(512-thread wide CTAs)");
   std::lock_guard<std::mutex> lk(p->mu);
   p->variant = min_ctas_per_sm;
+  return EMDB_OK;
+}
+
+int emdb_plan_set_max_ctas(emdb_plan* p, int max_ctas) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (max_ctas < 0) return fail(EMDB_ERR_INVALID, "max_ctas must be >= 0");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->max_ctas = max_ctas;
   return EMDB_OK;
 }
 

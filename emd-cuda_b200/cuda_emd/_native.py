@@ -26,7 +26,7 @@ STATUS_TOO_LONG = 2
 
 # Every symbol include/emdb200.h declares (checked by the CPU test suite).
 EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_set_arena",
-           "emdb_plan_set_variant",
+           "emdb_plan_set_variant", "emdb_plan_set_max_ctas",
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
@@ -66,6 +66,7 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_destroy.argtypes = [VP]
         L.emdb_plan_set_arena.argtypes = [VP, I]
         L.emdb_plan_set_variant.argtypes = [VP, I]
+        L.emdb_plan_set_max_ctas.argtypes = [VP, I]
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
@@ -187,6 +188,9 @@ class Plan:
 
     def set_variant(self, min_ctas_per_sm: int) -> None:
         check(self.L.emdb_plan_set_variant(self.handle, int(min_ctas_per_sm)), "emdb_plan_set_variant")
+
+    def set_max_ctas(self, max_ctas: int) -> None:
+        check(self.L.emdb_plan_set_max_ctas(self.handle, int(max_ctas)), "emdb_plan_set_max_ctas")
 
     def query(self, max_n: int) -> tuple[int, int, int]:
         a, c, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -98,13 +98,20 @@ class RaggedRunner:
     """Decompose CSR batches with per-tier launches (optionally graph-captured)."""
 
     def __init__(self, config: EMDKernelConfig | None = None, device: int | None = None,
-                 cache_path: str | None = DEFAULT_CACHE, autotune: bool = True):
+                 cache_path: str | None = DEFAULT_CACHE, autotune: bool = True,
+                 heavy_passes: float = 600.0, heavy_boost: float = 1.0):
         import torch
         self.cfg = config or EMDKernelConfig()
         self.device = torch.cuda.current_device() if device is None else int(device)
         self.cache_path = cache_path
         self.autotune = autotune
+        # learned tier choice: traces of a long tier predicted to need at least
+        # heavy_passes sift passes run in their own wide launch, on a share of
+        # the SMs (their predicted share of the work, times heavy_boost)
+        self.heavy_passes = float(heavy_passes)
+        self.heavy_boost = float(heavy_boost)
         self._tiers: dict[int, Tier] = {}
+        self._heavy_tiers: dict[int, Tier] = {}
         self._graph = None
         self._graph_key = None
         self._cache = self._load_cache()
@@ -222,7 +229,7 @@ class RaggedRunner:
             None, 1, order_dev.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
             dn.data_ptr(), de.data_ptr(), dz.data_ptr(), st), "emdb_run_ragged")
 
-    def prepare(self, values, offsets, cost=None, offsets_host=None):
+    def prepare(self, values, offsets, cost=None, offsets_host=None, heavy=None, cost_host=None):
         """Host-side plan: tiers and per-tier queue orders (device int32).
 
         The tiers, their tuning and one persistent order buffer per tier are
@@ -230,18 +237,22 @@ class RaggedRunner:
         captured graph reads those buffers); each call refills the buffers on
         the current stream: FIFO, or longest `cost` first (cost: per-trace
         work estimates, device tensor or host array).  ``offsets_host`` (the
-        same offsets in host memory) spares the device read-back."""
-        key = (offsets.data_ptr(), int(offsets.shape[0]), values.data_ptr())
+        same offsets in host memory) spares the device read-back.  ``heavy``
+        (host bool per trace, with ``cost_host``): those traces of each long
+        tier run in their own launch of the wide instance (split_heavy)."""
+        import hashlib
+        hkey = None if heavy is None else hashlib.sha1(np.packbits(heavy).tobytes()).hexdigest()
+        key = (offsets.data_ptr(), int(offsets.shape[0]), values.data_ptr(), hkey)
         cached = getattr(self, "_prep", None)
         if cached is None or cached[0] != key:
-            tiers, idx = self._prepare(values, offsets, offsets_host)
+            tiers, idx = self._prepare(values, offsets, offsets_host, heavy, cost_host)
             orders = [x.clone() for x in idx]
             self._prep = cached = (key, tiers, idx, orders)
         _, tiers, idx, orders = cached
         self._fill_orders(idx, orders, cost, values.device)
         return tiers, orders
 
-    def _prepare(self, values, offsets, offsets_host=None):
+    def _prepare(self, values, offsets, offsets_host=None, heavy=None, cost_host=None):
         import torch
         if offsets_host is not None:
             off_h = np.asarray(offsets_host)
@@ -250,8 +261,45 @@ class RaggedRunner:
         lengths = np.diff(off_h)
         tiers = self.tiers_for(lengths)
         self.tune(values, offsets, lengths, tiers)
+        if heavy is not None:
+            tiers = self.split_heavy(tiers, np.asarray(heavy, dtype=bool), cost_host)
         idx = [torch.from_numpy(t.idx.astype(np.int32)).to(values.device) for t in tiers]
         return tiers, idx
+
+    def split_heavy(self, tiers: list, heavy: np.ndarray, cost: np.ndarray | None) -> list:
+        """The learned tier choice: the heavy traces of each long tier that
+        runs the 128-thread instance move to a launch of the wide instance
+        (one 512-thread CTA per SM, knots on-chip) capped at their share of
+        the SMs; the rest stay in the tuned launch.  Launched first, so their
+        CTAs take their SMs before the light launch fills the others."""
+        import torch
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        c = np.ones(heavy.shape[0]) if cost is None else np.asarray(cost, dtype=np.float64)
+        total = float(c.sum()) or 1.0
+        out = []
+        for t in tiers:
+            if t.edge < WIDE_FROM or t.variant == WIDE:
+                out.append(t)
+                continue
+            h = t.idx[heavy[t.idx]]
+            if h.size == 0:
+                out.append(t)
+                continue
+            ht = self._heavy_tiers.get(t.edge)
+            if ht is None:
+                ht = Tier(t.edge, h, self.cfg, self.device)
+                ht.set_tuning(WIDE, 0)
+                self._heavy_tiers[t.edge] = ht
+            ht.idx = h
+            ht.max_n = t.max_n
+            share = float(c[h].sum()) / total * self.heavy_boost
+            ht.plan.set_max_ctas(int(min(max(1, round(share * sms)), h.size, sms)))
+            out.append(ht)
+            light = t.idx[~heavy[t.idx]]
+            if light.size:
+                t.idx = light
+                out.append(t)
+        return out
 
     @staticmethod
     def _fill_orders(idx, orders, cost, device) -> None:
@@ -302,18 +350,37 @@ class RaggedRunner:
         return outs
 
     def run_learned(self, values, offsets, model, outs=None, use_graph: bool = False,
-                    offsets_host=None):
+                    offsets_host=None, split_heavy: bool = False):
         """run() with the queue ordered longest-predicted-first by a cost model
         (cuda_emd.scheduler.CostModel): features and BF16 inference on the
-        device, per-tier order on the device, then the launches.  Same results
-        as FIFO, bit for bit."""
-        from . import scheduler as S
-        feats = S.features(values, offsets)
-        cost = S.predicted_cost(model, feats, offsets[1:] - offsets[:-1])
-        return self.run(values, offsets, cost=cost, outs=outs, use_graph=use_graph,
-                        offsets_host=offsets_host)
+        device, per-tier order on the device, then the launches.  With
+        split_heavy the model also picks the tier: traces it predicts to need
+        at least `heavy_passes` sift passes run on the wide instance
+        (split_heavy()).  Same results as FIFO, bit for bit."""
+        import torch
+        tiers, orders = self.prepare_learned(values, offsets, model, offsets_host, split_heavy)
+        with torch.cuda.nvtx.range("ragged launch"):
+            return self.launch(tiers, orders, values, offsets, outs, use_graph)
 
-    def run_host(self, values, offsets, model=None, use_graph: bool = True):
+    def prepare_learned(self, values, offsets, model, offsets_host=None, split_heavy=False):
+        """The learned step's planning: predicted cost per trace on the device,
+        and with split_heavy the heavy set on the host (one small read-back)."""
+        import torch
+        from . import scheduler as S
+        with torch.cuda.nvtx.range("ragged learned plan"):
+            feats = S.features(values, offsets)
+            lens = offsets[1:] - offsets[:-1]
+            pred = model.predict(feats)
+            cost = S.cost_from_prediction(pred, lens)
+            heavy = cost_h = None
+            if split_heavy:
+                passes = S.passes_from_prediction(pred)
+                both = torch.stack([passes, cost]).cpu().numpy()
+                heavy, cost_h = both[0] >= self.heavy_passes, both[1]
+            return self.prepare(values, offsets, cost, offsets_host, heavy, cost_h)
+
+    def run_host(self, values, offsets, model=None, use_graph: bool = True,
+                 split_heavy: bool = False):
         """Host CSR batch in, host results out (the end-to-end path): copy the
         traces up (page-locked inputs keep the copy asynchronous), order the
         queue by `model` if given (else FIFO), decompose, gather the rows that
@@ -353,7 +420,7 @@ class RaggedRunner:
             st["outs"] = self._alloc_out(v, o)
         if model is not None:
             outs = self.run_learned(v, o, model, outs=st["outs"], use_graph=use_graph,
-                                    offsets_host=off_np)
+                                    offsets_host=off_np, split_heavy=split_heavy)
         else:
             outs = self.run(v, o, outs=st["outs"], use_graph=use_graph, offsets_host=off_np)
         imfs, n_imfs, ovf, dn, de, dz = outs

@@ -200,15 +200,24 @@ class CostModel:
         return cm
 
 
+def passes_from_prediction(y):
+    """Predicted total sift passes per trace from the model's output."""
+    import torch
+    # 2^y as exp(y ln 2): torch's precompiled exp, where exp2 is compiled at run
+    # time on first use of each vector width (~0.4 s inside a timed step)
+    return torch.exp(y[:, 0] * 0.6931471805599453).clamp(min=1.0) - 1.0
+
+
+def cost_from_prediction(y, lengths):
+    """Work estimate per trace: N x predicted sift passes (only orders the
+    queue and picks the tier)."""
+    import torch
+    return lengths.to(torch.float32) * passes_from_prediction(y).clamp(min=1.0)
+
+
 def predicted_cost(model: CostModel, feats, lengths):
     """Work estimate per trace: N x predicted sift passes."""
-    import torch
-    y = model.predict(feats)
-    # 2^y as exp(y ln 2): torch's precompiled exp, where exp2 is compiled at run
-    # time on first use of each vector width (~0.4 s inside a timed step); the
-    # estimate only orders the queue
-    passes = torch.exp(y[:, 0] * 0.6931471805599453).clamp(min=1.0) - 1.0
-    return lengths.to(torch.float32) * passes.clamp(min=1.0)
+    return cost_from_prediction(model.predict(feats), lengths)
 
 
 def lpt_order(cost):

@@ -75,6 +75,12 @@ int emdb_plan_set_arena(emdb_plan* plan, int arena_bytes);
  * shared-memory arena, with the proto-IMF in global memory when shared
  * memory cannot hold it, so any trace length runs. */
 int emdb_plan_set_variant(emdb_plan* plan, int min_ctas_per_sm);
+/* Cap on the persistent grid of the plan's launches (0 = as many CTAs as
+ * can be resident).  A capped launch leaves the other SMs to launches that
+ * run beside it -- the learned scheduler gives the heavy traces of a tier a
+ * wide launch on a share of the SMs this way.  No reference counterpart (its
+ * grid is one CTA per signal, kernels.py:1366-1367). */
+int emdb_plan_set_max_ctas(emdb_plan* plan, int max_ctas);
 /* Arena and CTAs/SM the plan would use for traces up to max_n. */
 int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
                     int* grid_max);

@@ -113,3 +113,26 @@ def test_public_ragged_with_per_trace_time_axes():
         r = O.emd_signal(vals[offs[b]:offs[b + 1]], Tb)
         assert n_imfs[b] == r.n_imfs, b
         assert np.array_equal(imfs[16 * offs[b]:16 * offs[b + 1]].reshape(16, n), r.imfs), b
+
+
+def test_learned_tier_choice_changes_no_bit():
+    # the cost model also picks the tier: predicted-heavy traces of the long
+    # tiers run on the wide instance in their own capped launch; every output
+    # equals the FIFO single-tier run
+    import torch
+    from cuda_emd import EMDKernelConfig, scheduler as S
+    from cuda_emd.ragged import RaggedRunner
+    cfg = EMDKernelConfig(max_iteration=120)
+    vals, offs = _batch(160, 71, lo=1500, hi=8192)
+    v, o = torch.from_numpy(vals).cuda(), torch.from_numpy(offs).cuda()
+    ref = [x.clone() for x in cfg.build().run_ragged(v, o)]
+    cm = S.CostModel(seed=0)
+    cm.fit(S.features(v, o), S.labels_from_debug(ref[3], ref[1]), epochs=3, batch=64)
+    runner = RaggedRunner(cfg, cache_path=None, autotune=False, heavy_passes=50.0)
+    for graph in (False, True, True):
+        out = runner.run_learned(v, o, cm, use_graph=graph, offsets_host=offs, split_heavy=True)
+        torch.cuda.synchronize()
+        runner.check_status()
+        assert any(t.variant == 1 for t in runner._prep[1])     # some traces went wide
+        for a, b in zip(ref, out):
+            assert torch.equal(a, b)
