@@ -44,28 +44,42 @@ def _newer(src: list[str], dst: str) -> bool:
     return any(os.path.getmtime(s) > t for s in src if os.path.exists(s))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
-    os.makedirs(LIB_DIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, defines: list[str] | None = None,
+          out: str | None = None) -> str:
+    """Compile the units and link the library.  `defines` (e.g.
+    ["EMDB_LOAD_CLOCKS=1"]) and `out` build a variant library elsewhere,
+    with its objects in a build folder of its own (the product build is
+    unchanged)."""
+    defines = list(defines or [])
+    lib = out or LIB
+    bdir = BUILD if not defines else os.path.join(BUILD, "_".join(d.replace("=", "") for d in defines))
+    os.makedirs(bdir, exist_ok=True)
+    os.makedirs(os.path.dirname(lib), exist_ok=True)
     nvcc = _nvcc()
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "emdb200.h")]
     objs = []
     for src, extra in UNITS:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
+        o = os.path.join(bdir, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _newer([s, *hdrs, __file__], o):
-            cmd = [nvcc, *COMMON, *extra, "-c", s, "-o", o]
+            cmd = [nvcc, *COMMON, *extra, *[f"-D{d}" for d in defines], "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
             subprocess.run(cmd, check=True)
-    if force or _newer(objs, LIB):
-        cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"]
+    if force or _newer(objs, lib):
+        cmd = [nvcc, *ARCH, "-shared", "-o", lib, *objs, "-cudart", "static"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--define", action="append", default=[], help="extra -D for every unit")
+    ap.add_argument("--out", default=None, help="library path (default: lib/libemdb200.so)")
+    a = ap.parse_args()
+    print(build(force=a.force, verbose=True, defines=a.define, out=a.out))

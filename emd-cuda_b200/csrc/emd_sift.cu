@@ -122,6 +122,13 @@
 #ifndef EMDB_SORTED_NOCHECK
 #define EMDB_SORTED_NOCHECK 0
 #endif
+//  EMDB_LOAD_CLOCKS  instrumented build: thread 0 of each CTA adds the clock64
+//                  cycles of every trace's load into shared memory, and of
+//                  the whole trace, to the plan's counters [2] and [3]
+//                  (emdb_plan_phase_clocks); off in the product build
+#ifndef EMDB_LOAD_CLOCKS
+#define EMDB_LOAD_CLOCKS 0
+#endif
 
 namespace emdb {
 
@@ -1493,8 +1500,15 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     Ctl& C = *L.ctl;
     double* imf = L.imf;
     for (int k = tid; k < MAXI; k += NT) { C.dbg_n[k] = -1; C.dbg_e[k] = -1; C.dbg_z[k] = -1; }
+#if EMDB_LOAD_CLOCKS
+    const long long clk_trace0 = clock64();
+#endif
     for (int i = tid; i < N; i += NT) imf[i] = S[i];
     __syncthreads();
+#if EMDB_LOAD_CLOCKS
+    if (tid == 0 && p.counters)
+      atomicAdd(p.counters + 2, (unsigned long long)(clock64() - clk_trace0));
+#endif
 
     bool ovf = false;
     int imf_count = 0;
@@ -1676,6 +1690,10 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
       p.dbg_nzm[(int64_t)b * MAXI + k] = C.dbg_z[k];
     }
     __syncthreads();
+#if EMDB_LOAD_CLOCKS
+    if (tid == 0 && p.counters)
+      atomicAdd(p.counters + 3, (unsigned long long)(clock64() - clk_trace0));
+#endif
     // rows that may hold data: n_imfs, plus the dropped trend row that a
     // ~zero residue leaves in place (as the reference does)
     mark_trace_done(p, b, tid, nim + ((trend && rzero) ? 1 : 0));

@@ -13,7 +13,9 @@ import threading
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libemdb200.so")
+# EMDB_LIB overrides the library path (a measurement build, e.g. one with
+# EMDB_LOAD_CLOCKS=1); the default is the in-tree product build
+LIB_PATH = os.environ.get("EMDB_LIB") or os.path.join(os.path.dirname(HERE), "lib", "libemdb200.so")
 
 EMDB_OK = 0
 EMDB_ERR_INVALID = 1
@@ -26,7 +28,7 @@ STATUS_TOO_LONG = 2
 
 # Every symbol include/emdb200.h declares (checked by the CPU test suite).
 EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_set_arena",
-           "emdb_plan_set_variant", "emdb_plan_set_max_ctas",
+           "emdb_plan_set_variant", "emdb_plan_set_max_ctas", "emdb_plan_phase_clocks",
            "emdb_plan_query", "emdb_run", "emdb_run_ragged", "emdb_envelope", "emdb_status",
            "emdb_last_error", "emdb_features", "emdb_mlp_num_params", "emdb_mlp_forward",
            "emdb_mlp_backward", "emdb_mlp_adam", "emdb_mlp_infer_bf16", "emdb_check_division",
@@ -67,6 +69,8 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_set_arena.argtypes = [VP, I]
         L.emdb_plan_set_variant.argtypes = [VP, I]
         L.emdb_plan_set_max_ctas.argtypes = [VP, I]
+        L.emdb_plan_phase_clocks.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
+                                             ctypes.POINTER(ctypes.c_ulonglong), I]
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
@@ -216,6 +220,14 @@ class Plan:
         a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
         check(self.L.emdb_plan_counters(self.handle, ctypes.byref(a), ctypes.byref(b), int(reset)),
               "emdb_plan_counters")
+        return a.value, b.value
+
+    def phase_clocks(self, reset: bool = False) -> tuple[int, int]:
+        """(load cycles, trace cycles) summed over traces; non-zero only in a
+        library built with EMDB_LOAD_CLOCKS=1."""
+        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        check(self.L.emdb_plan_phase_clocks(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                            int(reset)), "emdb_plan_phase_clocks")
         return a.value, b.value
 
     def status(self, stream: int) -> int:

@@ -219,6 +219,14 @@ int emdb_run_noalloc(const emdb_config* cfg, const double* signals, const double
  * reference (its flags come back with each call's own buffers, emd.py:95-105). */
 int emdb_noalloc_status(int* status, void* stream);
 
+/* Cycles (clock64, summed over traces) spent loading each trace into shared
+ * memory and on the whole trace, recorded only by a library built with
+ * EMDB_LOAD_CLOCKS=1 (zeros otherwise): how much of a trace's time the load
+ * is.  Synchronises the device; reset != 0 clears them.  No reference
+ * counterpart (a measurement aid). */
+int emdb_plan_phase_clocks(emdb_plan* plan, unsigned long long* load_cycles,
+                           unsigned long long* trace_cycles, int reset);
+
 /* Synchronise `stream`, read and clear the plan's device status word
  * (EMDB_STATUS_* bits) into *status. */
 int emdb_status(emdb_plan* plan, int* status, void* stream);
