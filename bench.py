@@ -250,6 +250,8 @@ def main():
                     help="ragged64k: wide launches' SM share = predicted work share x this")
     ap.add_argument("--requests", type=int, default=160, help="serve: requests per load level")
     ap.add_argument("--loads", default="0.1,0.3,0.5,0.7,0.9,1.1", help="serve: offered loads")
+    ap.add_argument("--short-slots", type=int, default=2,
+                    help="serving: launch slots of the short-request lane (0 = one lane)")
     ap.add_argument("--serve-requests", type=int, default=160,
                     help="ragged64k: requests per load level of the serving sweep (0 = skip)")
     ap.add_argument("--serve-loads", default="0.3,0.7,1.1",
@@ -921,7 +923,7 @@ def run_ragged(a, rank, world, pool, cores):
         del plain_out, learned_out, plain_copy
         torch.cuda.empty_cache()
         serve = serve_sweep(cfg, local, cm, serve_traces,
-                            [float(x) for x in a.serve_loads.split(",")])
+                            [float(x) for x in a.serve_loads.split(",")], short_slots=a.short_slots)
     value = R.whole_job_rate(B, 1, world, learned_s)
     c = next((x for x in clk if x), None)
     if c and len(clk) > 1 and clk[1]:
@@ -995,7 +997,8 @@ def gen_requests(pool, nreq: int, seed0: int = 4000):
     return [t for chunk in res for t in chunk][:nreq]
 
 
-def serve_sweep(cfg, local: int, cm, traces: list, loads: list, slots: int = 4) -> dict:
+def serve_sweep(cfg, local: int, cm, traces: list, loads: list, slots: int = 4,
+                short_slots: int = 2) -> dict:
     """Continuous-batching server under Poisson arrivals: closed-loop
     saturation (every request at t=0), then each offered load as a fraction of
     it; p50/p99/p99.9 latency (delivery - arrival) per level."""
@@ -1003,8 +1006,9 @@ def serve_sweep(cfg, local: int, cm, traces: list, loads: list, slots: int = 4) 
     nreq = len(traces)
     mk = lambda: [Request(i, trs) for i, trs in enumerate(traces)]
     # warm-up (plans, kernels) and saturation
-    run_open_loop(EMDServer(cfg, local, slots=slots, cost_model=cm), mk()[:8], np.zeros(8))
-    sat = run_open_loop(EMDServer(cfg, local, slots=slots, cost_model=cm), mk(), np.zeros(nreq))
+    srv = lambda: EMDServer(cfg, local, slots=slots, short_slots=short_slots, cost_model=cm)
+    run_open_loop(srv(), mk()[:8], np.zeros(8))
+    sat = run_open_loop(srv(), mk(), np.zeros(nreq))
     sat_tps = sat["traces_per_s"]
     mean_tr = sum(len(t) for t in traces) / nreq
     rng = np.random.default_rng(77)
@@ -1013,12 +1017,12 @@ def serve_sweep(cfg, local: int, cm, traces: list, loads: list, slots: int = 4) 
         rate = load * sat_tps / mean_tr
         arr = poisson_arrivals(rate, nreq, rng)
         arr -= arr[0]
-        rep = run_open_loop(EMDServer(cfg, local, slots=slots, cost_model=cm), mk(), arr,
-                            timeout_s=900)
+        rep = run_open_loop(srv(), mk(), arr, timeout_s=900)
         rep.update({"offered_load": load, "offered_traces_per_s": round(load * sat_tps, 1)})
         levels.append({k: (round(v, 3) if isinstance(v, float) else v) for k, v in rep.items()})
     return {"desc": WORKLOADS["serve"]["desc"], "requests_per_level": nreq,
             "mean_traces_per_request": round(mean_tr, 2), "slots": slots,
+            "short_slots": short_slots,
             "order": "learned longest-predicted-first inside each admitted batch",
             "saturation": {"traces_per_s": round(sat_tps, 1), "p50_ms": round(sat["p50_ms"], 2),
                            "p99_ms": round(sat["p99_ms"], 2)},
@@ -1047,7 +1051,8 @@ def run_serve(a, rank, world, pool, cores):
     cm = S.CostModel(local, seed=0)
     cm.fit(S.features(tvd, tod), S.labels_from_debug(out[3], out[1]), epochs=a.epochs, batch=1024)
     del out, tvd, tod
-    sv = serve_sweep(cfg, local, cm, traces, [float(x) for x in a.loads.split(",")])
+    sv = serve_sweep(cfg, local, cm, traces, [float(x) for x in a.loads.split(",")],
+                     short_slots=a.short_slots)
     levels = sv["levels"]
     p99_90 = next((l["p99_ms"] for l in levels if abs(l["offered_load"] - 0.9) < 1e-6), None)
     line = {

@@ -237,18 +237,21 @@ int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
   int variant = p->variant;
   int arena = arena_for(p, max_n);
   bool gimf = false;
-  if (arena <= 0 || emdb::sift_fixed_smem(max_n, variant) + 64 > (size_t)arena) {
-    // Too long for the plan's instance: the wide instance at the full arena
+  if ((arena <= 0 || emdb::sift_fixed_smem(max_n, variant) + 64 > (size_t)arena) &&
+      p->arena_override == 0) {
+    // Too long for the plan's instance (at its automatic arena; an explicit
+    // arena that cannot hold the trace is the caller's error, below): the
+    // wide instance at the full arena
     // (the reference keeps whole traces in global memory, kernels.py:869-878,
     // so it has no length limit; neither does this fallback): the proto-IMF in
     // shared memory while it fits, else in the CTA's global slab.
     variant = 1;
     arena = p->smem_optin & ~127;
     gimf = emdb::sift_fixed_smem(max_n, 1) + 64 > (size_t)arena;
-    if (emdb::sift_fixed_smem(max_n, 1, gimf) + 64 > (size_t)arena)
-      return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
-                  " does not fit this device's shared memory");
   }
+  if (arena <= 0 || emdb::sift_fixed_smem(max_n, variant, gimf) + 64 > (size_t)arena)
+    return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
+                " does not fit this device's shared memory");
   int per_sm = 0;
   cudaError_t e = emdb::sift_occupancy(arena, variant, &per_sm, gimf);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
