@@ -204,6 +204,7 @@ class EMDServer:
         self.smem_sm = props.shared_memory_per_multiprocessor
         self.smem_optin = props.shared_memory_per_block_optin
         self.adaptive_arena = adaptive_arena
+        self.wide_from = 4096           # tiers this long may take the wide instances
         self.min_arena: dict[int, int] = {}
         self.nslots = slots + short_slots
         self.budget = int(hbm_budget_bytes)
@@ -310,6 +311,20 @@ class EMDServer:
             m = self.min_arena[edge] = self._plan(0, edge).min_arena(edge)
         return arena if arena >= m else 0
 
+    def _tier_instance(self, edge: int, in_flight: int) -> tuple[int, int]:
+        """(kernel variant, arena) of a tier launch.  A lightly loaded server
+        is latency-bound, so long traces get a whole SM each (the 512-thread
+        wide instance, 16 warps per trace, knots on-chip) while the traces in
+        flight fit one per SM, half an SM (two 256-thread CTAs) while they
+        fit two per SM; otherwise the 128-thread instance with the load-sized
+        arena of _tier_arena.  Results are the same bits whichever runs."""
+        if self.adaptive_arena and edge >= self.wide_from:
+            if in_flight <= self.num_sms:
+                return 1, 0
+            if in_flight <= 2 * self.num_sms:
+                return 2, 0
+        return 4, self._tier_arena(edge, in_flight)
+
     def _admit(self) -> int:
         """Admit pending requests into free slots of their lanes while the budget allows."""
         admitted = 0
@@ -369,7 +384,9 @@ class EMDServer:
             ts = self._tier_stream(slot, e)
             ts.wait_event(ready)
             p = self._plan(slot, e)
-            p.set_arena(self._tier_arena(e, in_flight))
+            variant, arena = self._tier_instance(e, in_flight)
+            p.set_variant(variant)
+            p.set_arena(arena)
             _native.check(p.L.emdb_run_ragged_notify(
                 p.handle, vals.data_ptr(), offs.data_ptr(), int(cnt), int(e), None, 1,
                 order.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),

@@ -119,3 +119,17 @@ def test_cancel_and_expire_waiting_requests():
     assert a.expire(6.0) == [r2] and r2.status == "timeout"
     b = a.next_batches(False)
     assert [r.rid for _, _, rs, _ in b for r in rs] == [0] and r0.status == "running"
+
+
+@pytest.mark.parametrize("in_flight,edge,want", [
+    (1, 8192, (1, 0)),             # one SM per trace: the 512-thread instance
+    (SM, 16384, (1, 0)),
+    (SM + 1, 8192, (2, 0)),        # two per SM: two 256-thread CTAs per SM
+    (2 * SM, 4096, (2, 0)),
+    (2 * SM + 1, 8192, (4, 0)),    # denser: the 128-thread instance, plan rule
+    (1, 2048, (4, OPTIN)),         # short tiers keep the 128-thread instance
+])
+def test_tier_instance_by_load(in_flight, edge, want):
+    s = _server(min_arena=MIN)
+    s.wide_from = 4096
+    assert s._tier_instance(edge, in_flight) == want
