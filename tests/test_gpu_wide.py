@@ -76,7 +76,7 @@ def test_wide_equals_narrow_on_long_overflowing_traces(N):
                         np.stack([W.chirp_trace(rng, N) for _ in range(2)]),
                         W.sinusoid_batch(3, N, seed=N + 2)])
     ref = _run(_launcher(cfg, variant=4), X)
-    assert ref[2][:5].all()                    # the seismic traces overflowed
+    assert ref[2][:5].any()                    # seismic traces past max_extrema
     full = 232448
     floor = cfg.build()._plan.min_arena(N) + 1024     # the wide fixed part is a little larger
     for arena in (full, (full + floor) // 2 & ~127, (floor + 8192) & ~127, (floor + 127) & ~127):
