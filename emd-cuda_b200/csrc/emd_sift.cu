@@ -123,12 +123,29 @@
 #define EMDB_SORTED_NOCHECK 0
 #endif
 //  EMDB_LOAD_CLOCKS  instrumented build: thread 0 of each CTA adds the clock64
-//                  cycles of every trace's load into shared memory, and of
-//                  the whole trace, to the plan's counters [2] and [3]
+//                  cycles of every trace's load into shared memory, of the
+//                  whole trace, and of each phase of the sift passes (taken at
+//                  the barriers that end them) to the plan's counters [2..]
 //                  (emdb_plan_phase_clocks); off in the product build
 #ifndef EMDB_LOAD_CLOCKS
 #define EMDB_LOAD_CLOCKS 0
 #endif
+#if EMDB_LOAD_CLOCKS
+// phases: 0 knot fill, 1 mirroring (+ parking), 2 spline rows, 3 PCR levels,
+// 4 diagonal solve, 5 evaluation / update, 6 lane sums, 7 reduction trees +
+// extrema scan, 8 per-IMF rows and reload, 9 the rest of the loop
+#define EMDB_PH(Cptr, k)                                      \
+  do {                                                        \
+    if (threadIdx.x == 0) {                                   \
+      const long long t_ = clock64();                         \
+      (Cptr)->ph[k] += (unsigned long long)(t_ - (Cptr)->ph_last); \
+      (Cptr)->ph_last = t_;                                   \
+    }                                                         \
+  } while (0)
+#else
+#define EMDB_PH(Cptr, k) do {} while (0)
+#endif
+constexpr int kPhases = 10;
 
 namespace emdb {
 
@@ -159,6 +176,10 @@ struct Ctl {
   int dbg_n[kMaxImfsCap], dbg_e[kMaxImfsCap], dbg_z[kMaxImfsCap];
   int chunk_bad;
   double sums[8];
+#if EMDB_LOAD_CLOCKS
+  unsigned long long ph[kPhases];
+  long long ph_last;
+#endif
 };
 
 // The 6 x 128 reduction lanes have no fixed home: between sift passes they sit
@@ -950,7 +971,7 @@ __device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* _
 
 template <int NT, bool kInt = false>
 __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kbase1, int kcnt0,
-                                              int kcnt1, int tid) {
+                                              int kcnt1, int tid, Ctl* C = nullptr) {
   const int m0 = kcnt0 >= 4 ? kcnt0 - 2 : 0;
   const int m1 = kcnt1 >= 4 ? kcnt1 - 2 : 0;
   const int mt = m0 + m1;
@@ -970,6 +991,7 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     P[r] = a; P[cap + r] = b; P[2 * cap + r] = c; P[3 * cap + r] = d;
   }
   __syncthreads();
+  if (C) EMDB_PH(C, 2);
   const int mmax = max(m0, m1);
   int cur = 0;
   int fin0 = 0, fin1 = 0;
@@ -999,6 +1021,7 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     // solve below does too, so those transitions keep the barrier.
     if (s < NT || 2 * s >= mmax) __syncthreads();
   }
+  if (C) EMDB_PH(C, 3);
   // diagonal solve + end-moment recovery (M[0], M[n-1] by the owners of the end rows)
   for (int r = tid; r < mt; r += NT) {
     const bool s0 = r < m0;
@@ -1027,6 +1050,7 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     }
   }
   __syncthreads();
+  if (C) EMDB_PH(C, 4);
 }
 
 // One PCR row update (kernels.py:651-668), in the reference's operation order.
@@ -1229,8 +1253,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
            : kPlace == kPlacePark   ? place_knots_park(imf, slab, N, kc0, kc1, L.red)
                                     : place_knots(slab, kc0, kc1);
   PassSums ps;
+  EMDB_PH(&C, 9);
   bool bad = fill_true_knots<NT>(L, K, e, N, NB, T, warp, lane);
   bad = __syncthreads_or(bad);
+  EMDB_PH(&C, 0);
   bool mbad = false;
   if (warp == 0) {
     mbad = mirror_both(L, K, e, N, NB, T, lane);
@@ -1244,8 +1270,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     for (int i = tid - 32; i < N; i += kThreads - 32) save[i] = imf[i];
   }
   ps.bad = __syncthreads_or(bad || mbad) != 0;
+  EMDB_PH(&C, 1);
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
-  solve_splines<NT, kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid);
+  solve_splines<NT, kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid,
+                                             EMDB_LOAD_CLOCKS ? &C : nullptr);
   const double* oldv = kWide ? park_old
                      : (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark)
                             ? borrow_save(slab) : imf;
@@ -1367,6 +1395,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   if (kWide) {
     // the reference's 128 lanes, each summing its samples in increasing order
     __syncthreads();
+    EMDB_PH(&C, 5);
     if (tid < kThreads) {
       for (int i = tid; i < N; i += kThreads) {
         const double old = oldv[i], nw = imf[i], qd = qbuf[i];
@@ -1387,6 +1416,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
   }
   __syncthreads();
+  EMDB_PH(&C, kWide ? 6 : 5);
 #if EMDB_TREE_SPLIT
   // the six trees spread over the warps (warp w: sum w; warps 0/1 also the
   // max / min tree); the next extrema scan's barrier publishes C.sums
@@ -1508,6 +1538,10 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
 #if EMDB_LOAD_CLOCKS
     if (tid == 0 && p.counters)
       atomicAdd(p.counters + 2, (unsigned long long)(clock64() - clk_trace0));
+    if (tid == 0) {
+      for (int k = 0; k < kPhases; ++k) C.ph[k] = 0;
+      C.ph_last = clock64();
+    }
 #endif
 
     bool ovf = false;
@@ -1584,6 +1618,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         stale |= (flags & 2) != 0;
         // ---- post-update extrema scan (also next pass's pre-scan) ----
         e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
+        EMDB_PH(&C, 7);
         ovf |= e.overflow;
         const int extNo2 = e.n_max + e.n_min;
         const int nzm2 = e.n_zer;
@@ -1604,6 +1639,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         }
       }
       // ---- emit IMF row, running residue into the next row, end condition ----
+      EMDB_PH(&C, 9);
       {
         const double* rsrc = imf_count == 0 ? S : out + (int64_t)imf_count * N;
         double* row = out + (int64_t)imf_count * N;
@@ -1640,6 +1676,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
         ovf |= e.overflow;
       }
+      EMDB_PH(&C, 8);
     }
 
     // ---- epilogue: trend removal, residue ~ 0 test, zero unused rows ----
@@ -1691,8 +1728,10 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     }
     __syncthreads();
 #if EMDB_LOAD_CLOCKS
-    if (tid == 0 && p.counters)
+    if (tid == 0 && p.counters) {
       atomicAdd(p.counters + 3, (unsigned long long)(clock64() - clk_trace0));
+      for (int k = 0; k < kPhases; ++k) atomicAdd(p.counters + 4 + k, C.ph[k]);
+    }
 #endif
     // rows that may hold data: n_imfs, plus the dropped trend row that a
     // ~zero residue leaves in place (as the reference does)

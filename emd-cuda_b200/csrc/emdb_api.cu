@@ -27,8 +27,9 @@ struct emdb_plan {
   int variant = 4;            // register-budget variant (min CTAs per SM)
   int max_ctas = 0;           // cap on a launch's persistent grid (0 = resident CTAs)
   int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
-  unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes,
-                                        // [2] / [3] load / trace cycles (instrumented build)
+  unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes, [2] / [3]
+                                        // load / trace cycles, [4..13] phase cycles
+                                        // (instrumented build)
   char* d_slab = nullptr;
   size_t slab_stride = 0;     // knot slab per CTA (the wide instance adds trace arrays)
   size_t slab_bytes = 0;      // allocated
@@ -67,6 +68,8 @@ struct emdb_notify {
 };
 
 namespace {
+
+constexpr int kCounters = 14;   // see emdb_plan::d_cnt
 
 thread_local std::string g_last_error;
 
@@ -336,13 +339,13 @@ int emdb_plan_create(const emdb_config* cfg, int device, emdb_plan** out) {
     return cuda_fail(e, "allocating plan control words");
   }
   cudaMemset(p->d_ctl, 0, 4 * sizeof(int));
-  e = cudaMalloc(&p->d_cnt, 4 * sizeof(unsigned long long));
+  e = cudaMalloc(&p->d_cnt, kCounters * sizeof(unsigned long long));
   if (e != cudaSuccess) {
     cudaFree(p->d_ctl);
     delete p;
     return cuda_fail(e, "allocating plan counters");
   }
-  cudaMemset(p->d_cnt, 0, 4 * sizeof(unsigned long long));
+  cudaMemset(p->d_cnt, 0, kCounters * sizeof(unsigned long long));
   *out = p;
   return EMDB_OK;
 }
@@ -859,18 +862,16 @@ int emdb_plan_counters(emdb_plan* p, unsigned long long* passes, unsigned long l
   return EMDB_OK;
 }
 
-int emdb_plan_phase_clocks(emdb_plan* p, unsigned long long* load_cycles,
-                           unsigned long long* trace_cycles, int reset) {
-  if (!p || !load_cycles || !trace_cycles) return fail(EMDB_ERR_INVALID, "NULL argument");
+int emdb_plan_phase_clocks(emdb_plan* p, unsigned long long* cycles, int n, int reset) {
+  if (!p || !cycles || n < 0) return fail(EMDB_ERR_INVALID, "bad arguments");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
-  unsigned long long h[2] = {0, 0};
+  unsigned long long h[kCounters - 2] = {};
   cudaError_t e = cudaDeviceSynchronize();
   if (e == cudaSuccess) e = cudaMemcpy(h, p->d_cnt + 2, sizeof(h), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess && reset) e = cudaMemset(p->d_cnt + 2, 0, sizeof(h));
   if (e != cudaSuccess) return cuda_fail(e, "phase clock read-back");
-  *load_cycles = h[0];
-  *trace_cycles = h[1];
+  for (int k = 0; k < n; ++k) cycles[k] = k < kCounters - 2 ? h[k] : 0ull;
   return EMDB_OK;
 }
 

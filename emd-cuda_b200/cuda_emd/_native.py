@@ -69,8 +69,7 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_set_arena.argtypes = [VP, I]
         L.emdb_plan_set_variant.argtypes = [VP, I]
         L.emdb_plan_set_max_ctas.argtypes = [VP, I]
-        L.emdb_plan_phase_clocks.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
-                                             ctypes.POINTER(ctypes.c_ulonglong), I]
+        L.emdb_plan_phase_clocks.argtypes = [VP, P, I, I]
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
@@ -222,13 +221,16 @@ class Plan:
               "emdb_plan_counters")
         return a.value, b.value
 
-    def phase_clocks(self, reset: bool = False) -> tuple[int, int]:
-        """(load cycles, trace cycles) summed over traces; non-zero only in a
+    PHASES = ("load", "trace", "fill", "mirror", "spline rows", "pcr", "diagonal", "evaluation",
+              "lane sums", "trees+scan", "per-IMF", "rest")
+
+    def phase_clocks(self, reset: bool = False) -> dict:
+        """Cycle counts by phase (emdb_plan_phase_clocks); non-zero only in a
         library built with EMDB_LOAD_CLOCKS=1."""
-        a, b = ctypes.c_ulonglong(), ctypes.c_ulonglong()
-        check(self.L.emdb_plan_phase_clocks(self.handle, ctypes.byref(a), ctypes.byref(b),
-                                            int(reset)), "emdb_plan_phase_clocks")
-        return a.value, b.value
+        buf = (ctypes.c_ulonglong * len(self.PHASES))()
+        check(self.L.emdb_plan_phase_clocks(self.handle, ctypes.cast(buf, ctypes.c_void_p),
+                                            len(self.PHASES), int(reset)), "emdb_plan_phase_clocks")
+        return dict(zip(self.PHASES, (int(v) for v in buf)))
 
     def status(self, stream: int) -> int:
         s = ctypes.c_int()

@@ -219,13 +219,15 @@ int emdb_run_noalloc(const emdb_config* cfg, const double* signals, const double
  * reference (its flags come back with each call's own buffers, emd.py:95-105). */
 int emdb_noalloc_status(int* status, void* stream);
 
-/* Cycles (clock64, summed over traces) spent loading each trace into shared
- * memory and on the whole trace, recorded only by a library built with
- * EMDB_LOAD_CLOCKS=1 (zeros otherwise): how much of a trace's time the load
- * is.  Synchronises the device; reset != 0 clears them.  No reference
- * counterpart (a measurement aid). */
-int emdb_plan_phase_clocks(emdb_plan* plan, unsigned long long* load_cycles,
-                           unsigned long long* trace_cycles, int reset);
+/* Cycle counts (clock64, summed over traces) recorded only by a library
+ * built with EMDB_LOAD_CLOCKS=1 (zeros otherwise): cycles[0] loading each
+ * trace into shared memory, [1] whole traces, [2..11] the sift-pass phases
+ * (knot fill, mirroring, spline rows, PCR levels, diagonal solve,
+ * evaluation / update, lane sums, reduction trees + extrema scan, per-IMF
+ * rows, the rest), thread 0's view taken at the barriers that end them.
+ * Writes n values.  Synchronises the device; reset != 0 clears them.  No
+ * reference counterpart (a measurement aid). */
+int emdb_plan_phase_clocks(emdb_plan* plan, unsigned long long* cycles, int n, int reset);
 
 /* Synchronise `stream`, read and clear the plan's device status word
  * (EMDB_STATUS_* bits) into *status. */
