@@ -82,7 +82,9 @@ WORKLOADS = {
     "sinusoid256": dict(n=256, N=1024, desc="256 three-tone traces x 1024 samples"),
     "seismic1k": dict(n=1024, N=2048, desc="1024 seismic traces x 2048 samples (profiling size)"),
     "seismic8k": dict(n=2048, N=8192, desc="2048 seismic traces x 8192 samples (every trace overflows "
-                                           "max_extrema; knots in the per-CTA slab)"),
+                                           "max_extrema)"),
+    "seismic8k-prof": dict(n=296, N=8192, desc="296 seismic traces x 8192 samples (two per SM: the "
+                                               "profiling size of seismic8k)"),
     "serve": dict(lo=512, hi=16384, max_traces=64,
                   desc="Poisson requests of 1-64 traces, N log-uniform [512, 16384], ragged mix; "
                        "offered load 10-110% of measured saturation"),
