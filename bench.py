@@ -61,9 +61,13 @@ METRIC_HEADLINE = ("EMD signals/s (FP64) learned-scheduled vs plain on one B200;
 # outputs are per trace and the spill slab stays in L2, so a launch's traffic
 # is this figure times its traces.
 NCU_DRAM_BYTES_PER_TRACE = {(2048, 16): 264329984 / 1024}
-# DRAM bytes per sample of the ragged mix's tier launches (None until captured)
-NCU_DRAM_BYTES_PER_SAMPLE_RAGGED = None
-NCU_RAGGED_SOURCE = None
+# DRAM bytes per sample of the ragged mix's tier launches: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum over the four tier launches of
+# a learned step on a 4,096-trace sample of the batch (9.30 M samples), mean
+# of 11 steps 1,120.8 MB: inputs and outputs are per sample, spills stay in L2
+NCU_DRAM_BYTES_PER_SAMPLE_RAGGED = 1120837888.0 / 9298408
+NCU_RAGGED_SOURCE = ("ncu dram__bytes_read+write of the tier launches of a 4096-trace "
+                     "sample of the batch (120.5 B/sample) x samples per step")
 
 
 def hbm_peak_gbs():
