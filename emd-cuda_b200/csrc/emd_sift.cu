@@ -89,6 +89,16 @@
 #ifndef EMDB_PCR_PAIR
 #define EMDB_PCR_PAIR 0
 #endif
+//  EMDB_WIDE_PCR_PAIR  the same for the wide (256 / 512-thread) instances
+#ifndef EMDB_WIDE_PCR_PAIR
+#define EMDB_WIDE_PCR_PAIR 0
+#endif
+//  EMDB_WIDE_OVERLAP  wide instances: the warps past the 128 reduction lanes
+//                  run the post-update extrema scan while the lanes sum the
+//                  stop-test terms (the scan then has NT/32 - 4 slots)
+#ifndef EMDB_WIDE_OVERLAP
+#define EMDB_WIDE_OVERLAP 1
+#endif
 #ifndef EMDB_OUTLINE
 #define EMDB_OUTLINE 2
 #endif
@@ -188,6 +198,18 @@ struct Ctl {
 // when those are smaller than the lanes).
 constexpr int kRedDoubles = 6 * kThreads;
 constexpr size_t kRedBytes = kRedDoubles * sizeof(double);
+
+// Extrema-scan slots of a CTA of NT threads: one contiguous range of 32-sample
+// chunks per slot, scanned by one warp and filled into knots by one warp.
+// The wide instances that overlap the scan with the lane sums scan with the
+// warps past the first four, so they have NT/32 - 4 slots.
+template <int NT>
+__host__ __device__ constexpr int scan_slots() {
+  return (NT > kThreads && EMDB_WIDE_OVERLAP) ? NT / 32 - kWarps : NT / 32;
+}
+// first warp that scans
+template <int NT>
+__host__ __device__ constexpr int scan_warp0() { return NT / 32 - scan_slots<NT>(); }
 
 // Per-warp scan counts (maxima, minima, sign changes, zero-run ends, fallback
 // trigger) live right after the control block: 5 x (warps per CTA) ints.
@@ -554,12 +576,12 @@ struct TimeAxis {
 // Extrema: count pass (find_extrema_parallel semantics, kernels.py:231-349,
 // with the serial scan's plateau rule, kernels.py:157-200).
 // ---------------------------------------------------------------------------
-template <int NT>
-__device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int warp, int lane) {
-  constexpr int NW = NT / 32;
+// NS slots; `slot` is the calling warp's slot.
+template <int NS>
+__device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int slot, int lane) {
   const double* imf = L.imf;
   int nch = (N + 31) >> 5;
-  int c0 = (warp * nch) / NW, c1 = ((warp + 1) * nch) / NW;
+  int c0 = (slot * nch) / NS, c1 = ((slot + 1) * nch) / NS;
   int rmax = 0, rmin = 0, zc = 0, zre = 0;
   bool trig = false;
   // neighbours straight from shared memory (conflict-free consecutive
@@ -605,8 +627,8 @@ __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int wa
   trig = __any_sync(kFull, trig);
   if (lane == 0) {
     int* w = L.wc;
-    w[warp] = rmax; w[NW + warp] = rmin;
-    w[2 * NW + warp] = zc; w[3 * NW + warp] = zre; w[4 * NW + warp] = trig ? 1 : 0;
+    w[slot] = rmax; w[NS + slot] = rmin;
+    w[2 * NS + slot] = zc; w[3 * NS + slot] = zre; w[4 * NS + slot] = trig ? 1 : 0;
   }
 }
 
@@ -623,9 +645,11 @@ struct ExtInfo {
 // find_extrema_parallel: without a fallback trigger the zero-crossing count is
 // sign changes only; with one, the serial count adds one per zero run that
 // ends before N (kernels.py:123-143, 273-276).
-template <int NT>
-__device__ __forceinline__ ExtInfo extrema_totals(const SmemLayout& L, int warp, int max_extrema) {
-  constexpr int NW = NT / 32;
+// `slot`: the caller's fill slot (its warp, if the warp fills), for its rank offsets
+template <int NS>
+__device__ __forceinline__ ExtInfo extrema_totals(const SmemLayout& L, int slot, int max_extrema) {
+  constexpr int NW = NS;
+  const int warp = slot;
   const Ctl& C = *L.ctl;
   const int* wc = L.wc;
   ExtInfo e;
@@ -672,33 +696,45 @@ __device__ void chunk_fallback_check(const SmemLayout& L, int N, int tid) {
 
 // One extrema scan = count pass + totals.  Ends after a barrier with every
 // thread holding the same totals.
+// The totals of a finished count pass (after its barrier), and the
+// reference's rare chunk fallback.  Every thread gets the totals; a warp that
+// fills gets its slot's rank offsets.
+template <int NT>
+__device__ __forceinline__ ExtInfo extrema_finish(const SmemLayout& L, int N, int tid, int warp,
+                                                  int max_extrema) {
+  constexpr int NS = scan_slots<NT>();
+  const int slot = warp < NS ? warp : 0;
+  ExtInfo e = extrema_totals<NS>(L, slot, max_extrema);
+  if (N > kThreads * 128 && L.imf[0] == 0.0 && !e.trig) {
+    chunk_fallback_check(L, N, tid);
+    e = extrema_totals<NS>(L, slot, max_extrema);
+  }
+  return e;
+}
+
 template <int NT>
 __device__ __forceinline__ ExtInfo extrema_scan(const SmemLayout& L, int N, int tid, int warp,
                                                 int lane, int max_extrema) {
-  extrema_count<NT>(L, N, warp, lane);
+  constexpr int W0 = scan_warp0<NT>();
+  if (W0 == 0 || warp >= W0) extrema_count<scan_slots<NT>()>(L, N, warp - W0, lane);
   if (tid == 0) L.ctl->chunk_bad = 0;
   __syncthreads();
-  ExtInfo e = extrema_totals<NT>(L, warp, max_extrema);
-  if (N > kThreads * 128 && L.imf[0] == 0.0 && !e.trig) {
-    chunk_fallback_check(L, N, tid);
-    e = extrema_totals<NT>(L, warp, max_extrema);
-  }
-  return e;
+  return extrema_finish<NT>(L, N, tid, warp, max_extrema);
 }
 
 // ---------------------------------------------------------------------------
 // Knot fill: compacted true extrema -> X/Y at offset NB (both sides).
 // Returns this thread's "bad envelope sign" vote for true knots.
 // ---------------------------------------------------------------------------
-template <int NT>
+// NS slots; the calling warp fills slot `warp` (warps past NS do not call it)
+template <int NS>
 __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots& K,
                                                 const ExtInfo& e, int N, int NB,
                                                 const TimeAxis& T, int warp, int lane) {
-  constexpr int NW = NT / 32;
   Ctl& C = *L.ctl;
   const double* imf = L.imf;
   int nch = (N + 31) >> 5;
-  int c0 = (warp * nch) / NW, c1 = ((warp + 1) * nch) / NW;
+  int c0 = (warp * nch) / NS, c1 = ((warp + 1) * nch) / NS;
   unsigned lt = (1u << lane) - 1u;
   bool bad = false;
   // one extremum lane: rank it, write its knot, note head / tail indices
@@ -999,8 +1035,9 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     const double* __restrict__ Pa = cur ? K.P[1] : K.P[0];
     double* __restrict__ Pn = cur ? K.P[0] : K.P[1];
     // two rows per trip: independent division chains overlap
-    for (int r = tid; r < mt; r += (1 + EMDB_PCR_PAIR) * NT) {
-      const int r2 = EMDB_PCR_PAIR ? r + NT : mt;
+    constexpr int kPair = NT > kThreads ? EMDB_WIDE_PCR_PAIR : EMDB_PCR_PAIR;
+    for (int r = tid; r < mt; r += (1 + kPair) * NT) {
+      const int r2 = kPair ? r + NT : mt;
       {
         const bool s0 = r < m0;
         const int mq = s0 ? m0 : m1;
@@ -1254,7 +1291,9 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
                                     : place_knots(slab, kc0, kc1);
   PassSums ps;
   EMDB_PH(&C, 9);
-  bool bad = fill_true_knots<NT>(L, K, e, N, NB, T, warp, lane);
+  constexpr int NS = scan_slots<NT>();
+  bool bad = false;
+  if (NS == NT / 32 || warp < NS) bad = fill_true_knots<NS>(L, K, e, N, NB, T, warp, lane);
   bad = __syncthreads_or(bad);
   EMDB_PH(&C, 0);
   bool mbad = false;
@@ -1393,7 +1432,9 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     }
   }
   if (kWide) {
-    // the reference's 128 lanes, each summing its samples in increasing order
+    // the reference's 128 lanes, each summing its samples in increasing order;
+    // meanwhile the other warps run the next pass's extrema count on the
+    // updated proto-IMF (both only read it)
     __syncthreads();
     EMDB_PH(&C, 5);
     if (tid < kThreads) {
@@ -1407,7 +1448,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
         ps.omax = fmax(ps.omax, old);
         ps.omin = fmin(ps.omin, old);
       }
+    } else if (EMDB_WIDE_OVERLAP) {
+      extrema_count<scan_slots<NT>()>(L, N, warp - scan_warp0<NT>(), lane);
     }
+    if (EMDB_WIDE_OVERLAP && tid == 0) C.chunk_bad = 0;
   }
   // per-lane partial sums, then the reference's 128-lane trees on warp 0
   double* red = kPlace == kPlaceSlab ? L.red : K.red;
@@ -1428,6 +1472,8 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       if (lane == 0) C.sums[4 + warp] = b;
     }
   }
+  // overlapped scan: this barrier publishes C.sums (the scan's would have)
+  if (kWide && EMDB_WIDE_OVERLAP) __syncthreads();
 #else
   if (warp == 0) {
     double a0 = lane_tree(red, lane, 0);
@@ -1616,8 +1662,10 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         ++passes;
         const bool pass_bad = (flags & 1) != 0;
         stale |= (flags & 2) != 0;
-        // ---- post-update extrema scan (also next pass's pre-scan) ----
-        e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
+        // ---- post-update extrema scan (also next pass's pre-scan); the
+        // wide instances ran its count inside the pass ----
+        if (kWide && EMDB_WIDE_OVERLAP) e = extrema_finish<NT>(L, N, tid, warp, p.max_extrema);
+        else e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
         EMDB_PH(&C, 7);
         ovf |= e.overflow;
         const int extNo2 = e.n_max + e.n_min;
@@ -1754,7 +1802,7 @@ __device__ __forceinline__ void envelope_pass(const SmemLayout& L, char* slab, c
   Ctl& C = *L.ctl;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
   Knots K = place_knots(kSmem ? L.arena : slab, kc0, kc1);
-  fill_true_knots<kThreads>(L, K, e, N, NB, T, warp, lane);
+  fill_true_knots<kWarps>(L, K, e, N, NB, T, warp, lane);
   __syncthreads();
   if (warp == 0) mirror_both(L, K, e, N, NB, T, lane);
   __syncthreads();
