@@ -95,9 +95,14 @@
 #endif
 //  EMDB_WIDE_OVERLAP  wide instances: the warps past the 128 reduction lanes
 //                  run the post-update extrema scan while the lanes sum the
-//                  stop-test terms (the scan then has NT/32 - 4 slots)
+//                  stop-test terms (the scan then has NT/32 - 4 slots).
+//                  Same bits; measured on B200 (best of two): 512 threads,
+//                  1024 x 8192 seismic 291.2 vs 292.3 ms, 2048 x 4096 50.9 vs
+//                  51.6 ms; 256 threads, 2048 x 4096 50.4 vs 46.4 ms (its
+//                  knot fill then has 4 warps of 8) -- so off.
+//  EMDB_WIDE_PCR_PAIR 1: 291.1 / 51.2 ms, no gain.
 #ifndef EMDB_WIDE_OVERLAP
-#define EMDB_WIDE_OVERLAP 1
+#define EMDB_WIDE_OVERLAP 0
 #endif
 #ifndef EMDB_OUTLINE
 #define EMDB_OUTLINE 2
