@@ -256,6 +256,8 @@ def main():
                     help="ragged64k: wide launches' SM share = predicted work share x this")
     ap.add_argument("--requests", type=int, default=160, help="serve: requests per load level")
     ap.add_argument("--loads", default="0.1,0.3,0.5,0.7,0.9,1.1", help="serve: offered loads")
+    ap.add_argument("--slots", type=int, default=4,
+                    help="serving: launch slots of the long-request lane")
     ap.add_argument("--short-slots", type=int, default=2,
                     help="serving: launch slots of the short-request lane (0 = one lane)")
     ap.add_argument("--serve-requests", type=int, default=160,
@@ -929,7 +931,8 @@ def run_ragged(a, rank, world, pool, cores):
         del plain_out, learned_out, plain_copy
         torch.cuda.empty_cache()
         serve = serve_sweep(cfg, local, cm, serve_traces,
-                            [float(x) for x in a.serve_loads.split(",")], short_slots=a.short_slots)
+                            [float(x) for x in a.serve_loads.split(",")], slots=a.slots,
+                            short_slots=a.short_slots)
     value = R.whole_job_rate(B, 1, world, learned_s)
     c = next((x for x in clk if x), None)
     if c and len(clk) > 1 and clk[1]:
@@ -1058,7 +1061,7 @@ def run_serve(a, rank, world, pool, cores):
     cm.fit(S.features(tvd, tod), S.labels_from_debug(out[3], out[1]), epochs=a.epochs, batch=1024)
     del out, tvd, tod
     sv = serve_sweep(cfg, local, cm, traces, [float(x) for x in a.loads.split(",")],
-                     short_slots=a.short_slots)
+                     slots=a.slots, short_slots=a.short_slots)
     levels = sv["levels"]
     p99_90 = next((l["p99_ms"] for l in levels if abs(l["offered_load"] - 0.9) < 1e-6), None)
     line = {
