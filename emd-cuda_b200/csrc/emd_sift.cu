@@ -104,6 +104,15 @@
 #ifndef EMDB_WIDE_OVERLAP
 #define EMDB_WIDE_OVERLAP 0
 #endif
+//  EMDB_LANE_UNROLL  wide instances: unroll factor of the lane-sum loops (the
+//                  loads of a lane's samples in flight at once).  With the
+//                  six sums split over the 128-lane groups, B200, 512 threads
+//                  1024 x 8192 seismic / 256 threads 2048 x 4096 (ms): 4:
+//                  296.7 / 47.5, 8: 290.0 / 47.5, 16: 289.9 / 46.8; the sums
+//                  on the first 128 threads only (no split): 293.0 / 46.7.
+#ifndef EMDB_LANE_UNROLL
+#define EMDB_LANE_UNROLL 16
+#endif
 #ifndef EMDB_OUTLINE
 #define EMDB_OUTLINE 2
 #endif
@@ -169,6 +178,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kScanUnroll = EMDB_SCAN_UNROLL;
 constexpr int kFillUnroll = EMDB_FILL_UNROLL;
+constexpr int kLaneUnroll = EMDB_LANE_UNROLL;
 
 // reference thresholds (kernels.py:81-85, 814, 1069)
 constexpr double kEnergyRatioThr = 0.2;
@@ -1219,6 +1229,69 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
   ps.omin = fmin(ps.omin, old);
 }
 
+// The wide instances' stop-test sums after the update (new values in imf[],
+// old ones in oldv[], quotients (new-old)/new in qbuf[]): the reference's 128
+// lanes, lane l adding samples l, l+128, ... in increasing order exactly as
+// accumulate() does.  The six sums are independent chains, so the CTA's
+// 128-thread groups take them apart -- 512 threads: Σnew² | Σdiff² |
+// Σold², max, min | Σquotient²; 256 threads: the first two | the rest --
+// and write the lanes' partials to red[128 * sum + l] for the trees.
+template <int NT>
+__device__ __forceinline__ void wide_lane_sums(double* red, const double* __restrict__ oldv,
+                                               const double* imf, const double* __restrict__ qbuf,
+                                               int N, int tid) {
+  constexpr int NG = NT / kThreads;
+  static_assert(NG == 2 || NG == 4, "wide instances have 256 or 512 threads");
+  const int g = tid / kThreads, l = tid % kThreads;
+  if (g == 0) {
+    double s = 0.0, s2 = 0.0;
+#pragma unroll kLaneUnroll
+    for (int i = l; i < N; i += kThreads) {
+      const double nw = imf[i];
+      s += nw * nw;
+      if (NG == 2) {
+        const double diff = nw - oldv[i];
+        s2 += diff * diff;
+      }
+    }
+    red[l] = s;
+    if (NG == 2) red[128 + l] = s2;
+  } else if (NG == 4 && g == 1) {
+    double s = 0.0;
+#pragma unroll kLaneUnroll
+    for (int i = l; i < N; i += kThreads) {
+      const double diff = imf[i] - oldv[i];
+      s += diff * diff;
+    }
+    red[128 + l] = s;
+  } else if (g == NG / 2) {
+    double s = 0.0, mx = -1e30, mn = 1e30, sq = 0.0;
+#pragma unroll kLaneUnroll
+    for (int i = l; i < N; i += kThreads) {
+      const double old = oldv[i];
+      s += old * old;
+      mx = fmax(mx, old);
+      mn = fmin(mn, old);
+      if (NG == 2) {
+        const double q = qbuf[i];
+        sq += q * q;
+      }
+    }
+    red[256 + l] = s;
+    red[512 + l] = mx;
+    red[640 + l] = mn;
+    if (NG == 2) red[384 + l] = sq;
+  } else if (NG == 4 && g == 3) {
+    double s = 0.0;
+#pragma unroll kLaneUnroll
+    for (int i = l; i < N; i += kThreads) {
+      const double q = qbuf[i];
+      s += q * q;
+    }
+    red[384 + l] = s;
+  }
+}
+
 // eval_seg for the time axis T = arange(N): knot positions (true and
 // mirrored) and sample times are integers, so A = (x1-t)/h and B = (t-x0)/h
 // are quotients of integers 0 <= a <= h.  For those, q0 = RN(a*y) with
@@ -1436,7 +1509,13 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       accumulate(ps, old, nw);
     }
   }
-  if (kWide) {
+  // per-lane partial sums, then the reference's 128-lane trees on warp 0
+  double* red = kPlace == kPlaceSlab ? L.red : K.red;
+  if constexpr (kWide && !EMDB_WIDE_OVERLAP) {
+    __syncthreads();
+    EMDB_PH(&C, 5);
+    wide_lane_sums<NT>(red, oldv, imf, qbuf, N, tid);
+  } else if (kWide) {
     // the reference's 128 lanes, each summing its samples in increasing order;
     // meanwhile the other warps run the next pass's extrema count on the
     // updated proto-IMF (both only read it)
@@ -1458,9 +1537,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     }
     if (EMDB_WIDE_OVERLAP && tid == 0) C.chunk_bad = 0;
   }
-  // per-lane partial sums, then the reference's 128-lane trees on warp 0
-  double* red = kPlace == kPlaceSlab ? L.red : K.red;
-  if (!kWide || tid < kThreads) {
+  if (!kWide || (EMDB_WIDE_OVERLAP && tid < kThreads)) {
     red[tid] = ps.sq; red[128 + tid] = ps.dsq; red[256 + tid] = ps.osq;
     red[384 + tid] = ps.std_; red[512 + tid] = ps.omax; red[640 + tid] = ps.omin;
   }

@@ -24,7 +24,7 @@ struct emdb_plan {
   int num_sms = 0;
   int smem_optin = 0;
   int arena_override = 0;
-  int variant = 4;            // register-budget variant (min CTAs per SM)
+  int variant = 0;            // kernel instance (register variant); 0 = by trace length
   int max_ctas = 0;           // cap on a launch's persistent grid (0 = resident CTAs)
   int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
   unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes, [2] / [3]
@@ -134,8 +134,21 @@ int auto_arena_for(int smem_optin, int variant, int nbsym, int max_n) {
   return need <= (size_t)smem_optin ? (int)((need + 15) & ~size_t(15)) : 0;
 }
 
+// The plan's kernel instance for traces up to max_n.  Unless one was set
+// (or an arena, which is sized for the 128-thread instance): four 128-thread
+// CTAs per SM up to 2048 samples, two 256-thread CTAs per SM up to 4096, one
+// 512-thread CTA per SM beyond.  Measured on B200, dense seismic batches,
+// 128 / 256 / 512 threads: 16,384 x 2048 68 / 80 / 110 ms; 2,048 x 4096 72.1
+// / 46.3 / 51.6 ms; 1,024 x 8192 491.6 / 360.4 / 292.4 ms (three-tone and
+// chirp traces of 4096-8192 samples gain 1.6-2.9x on the wide instance).
+int effective_variant(const emdb_plan* p, int max_n) {
+  if (p->variant != 0) return p->variant;
+  if (p->arena_override > 0) return 4;
+  return max_n > 4096 ? 1 : max_n > 2048 ? 2 : 4;
+}
+
 int auto_arena(const emdb_plan* p, int max_n) {
-  return auto_arena_for(p->smem_optin, p->variant, p->cfg.nbsym, max_n);
+  return auto_arena_for(p->smem_optin, effective_variant(p, max_n), p->cfg.nbsym, max_n);
 }
 
 int arena_for(const emdb_plan* p, int max_n) {
@@ -237,7 +250,7 @@ int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
   if (max_n > kMaxTraceLen)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
                 " exceeds the longest supported trace (131072 samples)");
-  int variant = p->variant;
+  int variant = effective_variant(p, max_n);
   int arena = arena_for(p, max_n);
   bool gimf = false;
   if ((arena <= 0 || emdb::sift_fixed_smem(max_n, variant) + 64 > (size_t)arena) &&
@@ -386,10 +399,10 @@ int emdb_plan_set_arena(emdb_plan* p, int arena_bytes) {
 
 int emdb_plan_set_variant(emdb_plan* p, int min_ctas_per_sm) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
-  if (!emdb::sift_variant_ok(min_ctas_per_sm))
+  if (min_ctas_per_sm != 0 && !emdb::sift_variant_ok(min_ctas_per_sm))
     return fail(EMDB_ERR_INVALID,
-                "variant must be 4, 5 or 6 (128-thread CTAs), 2 (256-thread CTAs) or 1 "
-                "(512-thread wide CTAs)");
+                "variant must be 4, 5 or 6 (128-thread CTAs), 2 (256-thread CTAs), 1 "
+                "(512-thread wide CTAs) or 0 (by trace length)");
   std::lock_guard<std::mutex> lk(p->mu);
   p->variant = min_ctas_per_sm;
   return EMDB_OK;
@@ -409,7 +422,7 @@ int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm,
   int arena = arena_for(p, max_n);
   int per_sm = 0;
   if (arena > 0) {
-    cudaError_t e = emdb::sift_occupancy(arena, p->variant, &per_sm);
+    cudaError_t e = emdb::sift_occupancy(arena, effective_variant(p, max_n), &per_sm);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   }
   if (arena_bytes) *arena_bytes = arena;
@@ -806,7 +819,11 @@ int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batc
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
   cudaStream_t st = (cudaStream_t)stream;
-  int arena = arena_for(p, N);
+  // the envelope kernel has 128-thread CTAs: the arena rule of that instance
+  // unless the plan names another
+  int arena = p->arena_override > 0 ? p->arena_override
+                                    : auto_arena_for(p->smem_optin, p->variant ? p->variant : 4,
+                                                     p->cfg.nbsym, N);
   if (arena <= 0 || emdb::sift_fixed_smem(N) + 64 > (size_t)arena)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length does not fit this device's shared memory");
   int per_sm = 0;

@@ -70,7 +70,9 @@ int emdb_plan_set_arena(emdb_plan* plan, int arena_bytes);
  * least that many resident per SM (register budget), the automatic arena
  * then targets that many CTAs; 1 = the wide instance, one 512-thread CTA per
  * SM working on one trace (long traces: 16 warps and the knots on-chip);
- * 2 = two 256-thread CTAs per SM; same results bit for bit.  Chosen by the autotuner.  A launch whose traces
+ * 2 = two 256-thread CTAs per SM; same results bit for bit; 0 (the default)
+ * = by trace length: 4 up to 2048 samples, 2 up to 4096, 1 beyond (4 when
+ * an arena was set).  The ragged autotuner sets one per tier.  A launch whose traces
  * do not fit the plan's instance runs on the wide instance at the full
  * shared-memory arena, with the proto-IMF in global memory when shared
  * memory cannot hold it, so any trace length runs. */

@@ -80,7 +80,9 @@ def test_noalloc_long_traces_use_the_slab():
     from cuda_emd import EMDKernelConfig, _native, workloads as W
     cfg = EMDKernelConfig(max_iteration=40)          # keeps the test short
     X = torch.from_numpy(W.seismic_batch(6, 8192, seed=905)).cuda()
-    arena, _, _ = cfg.build()._plan.query(8192)
+    plan = cfg.build()._plan
+    plan.set_variant(4)                              # the no-allocation entry's instance
+    arena, _, _ = plan.query(8192)
     assert _native.pass_placement(cfg.to_c(), 8192, arena, cfg.max_extrema, cfg.max_extrema) in (2, 4)
     ref = _two_calls_equal(X, cfg=cfg)
     assert int(ref[2].sum()) == X.shape[0]           # every trace overflowed
