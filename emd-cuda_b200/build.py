@@ -22,13 +22,15 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH, f"-I{INCLUDE}"]
-# (source, extra flags)
+# (source, extra flags, object name)
 UNITS = [
-    ("emd_sift.cu", ["-fmad=false"]),
-    ("emd_sched.cu", []),
-    ("emdb_api.cu", []),
-    ("emdb_noalloc.cu", []),
-    ("emdb_pack.cu", []),
+    ("emd_sift.cu", ["-fmad=false"], "emd_sift"),
+    # the same kernels computing in float (namespace emdb::f32)
+    ("emd_sift.cu", ["-fmad=false", "-DEMDB_F32=1"], "emd_sift_f32"),
+    ("emd_sched.cu", [], "emd_sched"),
+    ("emdb_api.cu", [], "emdb_api"),
+    ("emdb_noalloc.cu", [], "emdb_noalloc"),
+    ("emdb_pack.cu", [], "emdb_pack"),
 ]
 HEADERS = ["emdb_internal.cuh", "emdb_sched.cuh"]
 
@@ -58,9 +60,9 @@ def build(force: bool = False, verbose: bool = False, defines: list[str] | None 
     nvcc = _nvcc()
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "emdb200.h")]
     objs = []
-    for src, extra in UNITS:
+    for src, extra, name in UNITS:
         s = os.path.join(CSRC, src)
-        o = os.path.join(bdir, os.path.splitext(src)[0] + ".o")
+        o = os.path.join(bdir, name + ".o")
         objs.append(o)
         if force or _newer([s, *hdrs, __file__], o):
             cmd = [nvcc, *COMMON, *extra, *[f"-D{d}" for d in defines], "-c", s, "-o", o]

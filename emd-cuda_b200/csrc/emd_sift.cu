@@ -171,7 +171,26 @@
 #endif
 constexpr int kPhases = 10;
 
+// EMDB_F32: the FP32 build of this file (namespace emdb::f32).  Every value
+// the sift computes is a `real`; the reference kernel's double literals keep
+// their C++ meaning, so float expressions that mix them are evaluated in
+// double and rounded once, as in the reference source compiled with REAL_T =
+// float.  The FP64 build's division shortcuts (reciprocal tables, Markstein
+// and branch-free quotients) are off: float quotients are the IEEE ones.
+#ifndef EMDB_F32
+#define EMDB_F32 0
+#endif
+#if EMDB_F32
+#undef EMDB_FAST_DIV
+#define EMDB_FAST_DIV 0
+#undef EMDB_PCR_NB
+#define EMDB_PCR_NB 0
+namespace emdb::f32 {
+using real = float;
+#else
 namespace emdb {
+using real = double;
+#endif
 
 namespace {
 
@@ -180,12 +199,13 @@ constexpr int kScanUnroll = EMDB_SCAN_UNROLL;
 constexpr int kFillUnroll = EMDB_FILL_UNROLL;
 constexpr int kLaneUnroll = EMDB_LANE_UNROLL;
 
-// reference thresholds (kernels.py:81-85, 814, 1069)
-constexpr double kEnergyRatioThr = 0.2;
-constexpr double kStdThr = 0.2;
-constexpr double kSvarThr = 0.001;
-constexpr double kTotalPowerThr = 0.005;
-constexpr double kRangeThr = 0.001;
+// reference thresholds (kernels.py:81-85, 814, 1069): the first five are
+// REAL_T functions there, the last two double literals compared with REAL_T
+constexpr real kEnergyRatioThr = 0.2;
+constexpr real kStdThr = 0.2;
+constexpr real kSvarThr = 0.001;
+constexpr real kTotalPowerThr = 0.005;
+constexpr real kRangeThr = 0.001;
 constexpr double kSumNewSqMin = 1e-10;
 constexpr double kResidueZeroAtol = 1e-8;
 constexpr int kLocalExtBuf = 64;  // kernels.py:206 (serial-fallback trigger)
@@ -200,7 +220,7 @@ struct Ctl {
   int kbase[2], kcnt[2];
   int dbg_n[kMaxImfsCap], dbg_e[kMaxImfsCap], dbg_z[kMaxImfsCap];
   int chunk_bad;
-  double sums[8];
+  real sums[8];
 #if EMDB_LOAD_CLOCKS
   unsigned long long ph[kPhases];
   long long ph_last;
@@ -212,7 +232,7 @@ struct Ctl {
 // reuse PCR buffer 1, which is dead from then on (or follow the PCR buffers
 // when those are smaller than the lanes).
 constexpr int kRedDoubles = 6 * kThreads;
-constexpr size_t kRedBytes = kRedDoubles * sizeof(double);
+constexpr size_t kRedBytes = kRedDoubles * sizeof(real);
 
 // Extrema-scan slots of a CTA of NT threads: one contiguous range of 32-sample
 // chunks per slot, scanned by one warp and filled into knots by one warp.
@@ -231,8 +251,8 @@ __host__ __device__ constexpr int scan_warp0() { return NT / 32 - scan_slots<NT>
 struct SmemLayout {
   Ctl* ctl;
   int* wc;            // [5][NW]: w_max | w_min | w_zc | w_zre | w_trig
-  double* red;        // [6][128] between passes (= arena start)
-  double* imf;        // [N]
+  real* red;        // [6][128] between passes (= arena start)
+  real* imf;        // [N]
   uint32_t* mmax;     // [nch] ballot masks of the last extrema scan
   uint32_t* mmin;
   uint16_t* pmax;     // per-chunk exclusive prefix within the owning warp's range
@@ -250,14 +270,14 @@ template <int NT = kThreads, bool kGImf = false>
 __host__ __device__ inline size_t fixed_bytes(int N) {
   size_t nch = (size_t)(N + 31) / 32;
   size_t b = align16(sizeof(Ctl)) + align16(5 * (NT / 32) * sizeof(int));
-  if (!kGImf) b += align16((size_t)N * sizeof(double));
+  if (!kGImf) b += align16((size_t)N * sizeof(real));
   b += align16(nch * 4) * 2 + align16(nch * 2) * 2;
   return b;
 }
 
 template <int NT = kThreads, bool kGImf = false>
 __device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total,
-                                            double* gimf = nullptr) {
+                                            real* gimf = nullptr) {
   SmemLayout L;
   size_t nch = (size_t)(N + 31) / 32;
   char* p = base;
@@ -272,10 +292,10 @@ __device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total,
   if (kGImf) {
     L.imf = gimf;
   } else {
-    L.imf = reinterpret_cast<double*>(p); p += align16((size_t)N * sizeof(double));
+    L.imf = reinterpret_cast<real*>(p); p += align16((size_t)N * sizeof(real));
   }
   L.arena = p;
-  L.red = reinterpret_cast<double*>(p);
+  L.red = reinterpret_cast<real*>(p);
   L.arena_bytes = arena_total - (int)(p - base);
   return L;
 }
@@ -285,12 +305,12 @@ __device__ __forceinline__ SmemLayout carve(char* base, int N, int arena_total,
 // moments M go into buffer 0's a (upper envelope) and c (lower) arrays and the
 // segment reciprocals R into buffer 1's a and c arrays.
 struct Knots {
-  double* X[2];
-  double* Y[2];
-  double* M[2];
-  double* R[2];   // RN(1/h) per knot segment, in buffer 1's a / c arrays
-  double* P[2];   // ping-pong PCR buffers: a | b | c | d, each `cap` rows
-  double* red;    // reduction lanes after the solve: buffer 1, or just past it
+  real* X[2];
+  real* Y[2];
+  real* M[2];
+  real* R[2];   // RN(1/h) per knot segment, in buffer 1's a / c arrays
+  real* P[2];   // ping-pong PCR buffers: a | b | c | d, each `cap` rows
+  real* red;    // reduction lanes after the solve: buffer 1, or just past it
   int cap;
 };
 
@@ -299,12 +319,12 @@ __host__ __device__ inline size_t knot_bytes(int kc0, int kc1) {
   const size_t cap = (size_t)kc0 + (size_t)kc1;
   // with EMDB_FAST_DIV 1 buffer 1 holds the segment reciprocals during evaluation
   const size_t red_extra = (EMDB_FAST_DIV != 1 && 4 * cap >= (size_t)kRedDoubles) ? 0 : kRedBytes;
-  return (2 * cap + 8 * cap) * sizeof(double) + red_extra;
+  return (2 * cap + 8 * cap) * sizeof(real) + red_extra;
 }
 
 __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
   Knots K;
-  double* p = reinterpret_cast<double*>(base);
+  real* p = reinterpret_cast<real*>(base);
   K.X[0] = p; p += kc0;
   K.Y[0] = p; p += kc0;
   K.X[1] = p; p += kc1;
@@ -325,20 +345,20 @@ __device__ __forceinline__ Knots place_knots(char* base, int kc0, int kc1) {
 // moments) in the arena, buffer 1 in the per-CTA global slab.  Evaluation then
 // reads shared memory only, and half of the PCR levels read the slab.
 __host__ __device__ inline size_t split_bytes(int kc0, int kc1) {
-  return 6 * ((size_t)kc0 + (size_t)kc1) * sizeof(double);
+  return 6 * ((size_t)kc0 + (size_t)kc1) * sizeof(real);
 }
 
 __device__ __forceinline__ Knots place_knots_split(char* sbase, int sbytes, char* gbase, int kc0,
                                                    int kc1) {
   Knots K;
-  double* p = reinterpret_cast<double*>(sbase);
+  real* p = reinterpret_cast<real*>(sbase);
   K.X[0] = p; p += kc0;
   K.Y[0] = p; p += kc0;
   K.X[1] = p; p += kc1;
   K.Y[1] = p; p += kc1;
   K.cap = kc0 + kc1;
   K.P[0] = p; p += 4 * K.cap;
-  K.P[1] = reinterpret_cast<double*>(gbase);
+  K.P[1] = reinterpret_cast<real*>(gbase);
   K.M[0] = K.P[0];
   K.M[1] = K.P[0] + 2 * K.cap;
   K.R[0] = K.P[1];
@@ -359,19 +379,19 @@ __device__ __forceinline__ Knots place_knots_split(char* sbase, int sbytes, char
 __host__ __device__ inline bool borrow_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
                                             int kc1) {
   const size_t cap = (size_t)kc0 + (size_t)kc1;
-  const size_t region = align16((size_t)N * sizeof(double)) + (size_t)arena_bytes;
-  return EMDB_FAST_DIV != 1 && 6 * cap * sizeof(double) <= (size_t)arena_bytes &&
-         10 * cap * sizeof(double) <= region &&
-         (align16((size_t)N * sizeof(double)) + kRedBytes) <= slab_stride;
+  const size_t region = align16((size_t)N * sizeof(real)) + (size_t)arena_bytes;
+  return EMDB_FAST_DIV != 1 && 6 * cap * sizeof(real) <= (size_t)arena_bytes &&
+         10 * cap * sizeof(real) <= region &&
+         (align16((size_t)N * sizeof(real)) + kRedBytes) <= slab_stride;
 }
 
-__device__ __forceinline__ double* borrow_save(char* slab) { return reinterpret_cast<double*>(slab); }
+__device__ __forceinline__ real* borrow_save(char* slab) { return reinterpret_cast<real*>(slab); }
 
-__device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, int arena_bytes,
+__device__ __forceinline__ Knots place_knots_borrow(real* imf, char* arena, int arena_bytes,
                                                     char* slab, int N, int kc0, int kc1) {
   Knots K;
   K.cap = kc0 + kc1;
-  double* p = reinterpret_cast<double*>(arena + arena_bytes) - 6 * K.cap;
+  real* p = reinterpret_cast<real*>(arena + arena_bytes) - 6 * K.cap;
   K.X[0] = p; p += kc0;
   K.Y[0] = p; p += kc0;
   K.X[1] = p; p += kc1;
@@ -382,7 +402,7 @@ __device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, in
   K.M[1] = K.P[0] + 2 * K.cap;
   K.R[0] = K.P[1];
   K.R[1] = K.P[1] + 2 * K.cap;
-  K.red = reinterpret_cast<double*>(slab + align16((size_t)N * sizeof(double)));
+  K.red = reinterpret_cast<real*>(slab + align16((size_t)N * sizeof(real)));
   return K;
 }
 
@@ -396,17 +416,17 @@ __device__ __forceinline__ Knots place_knots_borrow(double* imf, char* arena, in
 __host__ __device__ inline bool borrow2_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
                                              int kc1) {
   const size_t cap = (size_t)kc0 + (size_t)kc1;
-  const size_t region = align16((size_t)N * sizeof(double)) + (size_t)arena_bytes;
-  return EMDB_FAST_DIV != 1 && 3 * cap * sizeof(double) <= (size_t)arena_bytes &&
-         11 * cap * sizeof(double) <= region &&
-         (align16((size_t)N * sizeof(double)) + kRedBytes) <= slab_stride;
+  const size_t region = align16((size_t)N * sizeof(real)) + (size_t)arena_bytes;
+  return EMDB_FAST_DIV != 1 && 3 * cap * sizeof(real) <= (size_t)arena_bytes &&
+         11 * cap * sizeof(real) <= region &&
+         (align16((size_t)N * sizeof(real)) + kRedBytes) <= slab_stride;
 }
 
-__device__ __forceinline__ Knots place_knots_borrow2(double* imf, char* arena, int arena_bytes,
+__device__ __forceinline__ Knots place_knots_borrow2(real* imf, char* arena, int arena_bytes,
                                                      char* slab, int N, int kc0, int kc1) {
   Knots K;
   K.cap = kc0 + kc1;
-  double* p = reinterpret_cast<double*>(arena + arena_bytes) - 3 * K.cap;
+  real* p = reinterpret_cast<real*>(arena + arena_bytes) - 3 * K.cap;
   K.X[0] = p; p += kc0;
   K.Y[0] = p; p += kc0;
   K.X[1] = p; p += kc1;
@@ -417,7 +437,7 @@ __device__ __forceinline__ Knots place_knots_borrow2(double* imf, char* arena, i
   K.P[1] = imf + 4 * K.cap;
   K.R[0] = K.P[1];
   K.R[1] = K.P[1] + 2 * K.cap;
-  K.red = reinterpret_cast<double*>(slab + align16((size_t)N * sizeof(double)));
+  K.red = reinterpret_cast<real*>(slab + align16((size_t)N * sizeof(real)));
   return K;
 }
 
@@ -432,16 +452,16 @@ __device__ __forceinline__ Knots place_knots_borrow2(double* imf, char* arena, i
 __host__ __device__ inline bool park_fits(int N, int arena_bytes, size_t slab_stride, int kc0,
                                           int kc1) {
   const size_t cap = (size_t)kc0 + (size_t)kc1;
-  const size_t imfb = align16((size_t)N * sizeof(double));
-  return EMDB_FAST_DIV != 1 && 4 * cap * sizeof(double) <= imfb + (size_t)arena_bytes &&
-         imfb + 6 * cap * sizeof(double) <= slab_stride;
+  const size_t imfb = align16((size_t)N * sizeof(real));
+  return EMDB_FAST_DIV != 1 && 4 * cap * sizeof(real) <= imfb + (size_t)arena_bytes &&
+         imfb + 6 * cap * sizeof(real) <= slab_stride;
 }
 
-__device__ __forceinline__ Knots place_knots_park(double* imf, char* slab, int N, int kc0, int kc1,
-                                                  double* red) {
+__device__ __forceinline__ Knots place_knots_park(real* imf, char* slab, int N, int kc0, int kc1,
+                                                  real* red) {
   Knots K;
   K.cap = kc0 + kc1;
-  double* p = reinterpret_cast<double*>(slab + align16((size_t)N * sizeof(double)));
+  real* p = reinterpret_cast<real*>(slab + align16((size_t)N * sizeof(real)));
   K.X[0] = p; p += kc0;
   K.Y[0] = p; p += kc0;
   K.X[1] = p; p += kc1;
@@ -501,9 +521,9 @@ __device__ __noinline__ double div_slow(double a, double b) { return a / b; }
 // the fast quotients' range, knot lists that are not strictly increasing) as
 // calls to one out-of-line body each, instead of an inline copy per call site:
 // keeps the hot loops' code small.  Defined after eval_seg / search_seg.
-__device__ __noinline__ double eval_seg_cold(const double* x, const double* y, const double* M,
-                                             int n, double t, int lo);
-__device__ __noinline__ int search_seg_cold(const double* x, int n, double t);
+__device__ __noinline__ real eval_seg_cold(const real* x, const real* y, const real* M,
+                                             int n, real t, int lo);
+__device__ __noinline__ int search_seg_cold(const real* x, int n, real t);
 #if EMDB_OUTLINE >= 1
 #define EMDB_EVAL_RARE(sv, t, lo) eval_seg_cold((sv).x, (sv).y, (sv).M, (sv).n, (t), (lo))
 #define EMDB_SEARCH_RARE(sv, t) search_seg_cold((sv).x, (sv).n, (t))
@@ -562,11 +582,13 @@ __device__ __forceinline__ double div_nb(double a, double b, bool& slow) {
 }
 #endif
 
+#if !EMDB_F32
 __device__ __forceinline__ double div_rn(double a, double b, double y) {
   bool slow = false;
   const double q = div_q(a, b, y, slow);
   return slow ? div_slow(a, b) : q;
 }
+#endif
 constexpr double kInv6 = 1.0 / 6.0;   // RN(1/6), folded at compile time
 
 // RN(1/h) for integer h in [1, kRcpTab], built at compile time by IEEE
@@ -582,9 +604,9 @@ __device__ const RcpTab g_rcp = make_rcp_tab();
 
 
 struct TimeAxis {
-  const double* T;
+  const real* T;
   bool arange;
-  __device__ __forceinline__ double operator()(int i) const { return arange ? (double)i : T[i]; }
+  __device__ __forceinline__ real operator()(int i) const { return arange ? (real)i : T[i]; }
 };
 
 // ---------------------------------------------------------------------------
@@ -594,7 +616,7 @@ struct TimeAxis {
 // NS slots; `slot` is the calling warp's slot.
 template <int NS>
 __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int slot, int lane) {
-  const double* imf = L.imf;
+  const real* imf = L.imf;
   int nch = (N + 31) >> 5;
   int c0 = (slot * nch) / NS, c1 = ((slot + 1) * nch) / NS;
   int rmax = 0, rmin = 0, zc = 0, zre = 0;
@@ -604,11 +626,11 @@ __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int sl
 #pragma unroll kScanUnroll
   for (int c = c0; c < c1; ++c) {
     int i = (c << 5) + lane;
-    double v = (i < N) ? imf[i] : 0.0;
-    double vp = (i >= 1 && i - 1 < N) ? imf[i - 1] : 0.0;
-    double vn = (i + 1 < N) ? imf[i + 1] : 0.0;
+    real v = (i < N) ? imf[i] : 0.0;
+    real vp = (i >= 1 && i - 1 < N) ? imf[i - 1] : 0.0;
+    real vn = (i + 1 < N) ? imf[i + 1] : 0.0;
     bool interior = (i >= 1) && (i <= N - 2);
-    double dp = v - vp, dn = vn - v;
+    real dp = v - vp, dn = vn - v;
     bool strict = interior && (dp * dn < 0.0);
     bool ismin = strict && (dp < 0.0);
     bool ismax = strict && !(dp < 0.0);
@@ -619,7 +641,7 @@ __device__ __forceinline__ void extrema_count(const SmemLayout& L, int N, int sl
         int j = i;
         while (j + 1 < N && imf[j + 1] == v) ++j;
         if (j + 1 < N) {
-          double da = imf[j + 1] - imf[j];
+          real da = imf[j + 1] - imf[j];
           if (dp > 0.0 && da < 0.0) ismax = true;
           else if (dp < 0.0 && da > 0.0) ismin = true;
         }
@@ -695,13 +717,13 @@ __device__ __forceinline__ ExtInfo extrema_totals(const SmemLayout& L, int slot,
 // 128 threads' (threads past 128 of a wider CTA have none).  Ends with a barrier.
 __device__ void chunk_fallback_check(const SmemLayout& L, int N, int tid) {
   Ctl& C = *L.ctl;
-  const double* s = L.imf;
+  const real* s = L.imf;
   int cs = (N + kThreads - 1) / kThreads;
   int start = tid * cs, end = min(start + cs, N);
   int lo = max(start, 1), hi = min(end, N - 1);
   int nmx = 0, nmn = 0;
   for (int i = lo; i < hi; ++i) {
-    double dp = s[i] - s[i - 1], dn = s[i + 1] - s[i];
+    real dp = s[i] - s[i - 1], dn = s[i + 1] - s[i];
     if (dp * dn < 0.0) { if (dp < 0.0) ++nmn; else ++nmx; }
   }
   int bad = __syncthreads_or(nmx > kLocalExtBuf || nmn > kLocalExtBuf);
@@ -747,21 +769,21 @@ __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots
                                                 const ExtInfo& e, int N, int NB,
                                                 const TimeAxis& T, int warp, int lane) {
   Ctl& C = *L.ctl;
-  const double* imf = L.imf;
+  const real* imf = L.imf;
   int nch = (N + 31) >> 5;
   int c0 = (warp * nch) / NS, c1 = ((warp + 1) * nch) / NS;
   unsigned lt = (1u << lane) - 1u;
   bool bad = false;
   // one extremum lane: rank it, write its knot, note head / tail indices
-  auto put = [&](uint32_t bm, uint32_t bn, int pm, int pn, int ii, double v) {
+  auto put = [&](uint32_t bm, uint32_t bn, int pm, int pn, int ii, real v) {
     const bool ismax = (bm >> lane) & 1u;
     int q = ismax ? 0 : 1;
     int rank = q == 0 ? e.off_max + pm + __popc(bm & lt)
                       : e.off_min + pn + __popc(bn & lt);
     int nq = q == 0 ? e.n_max : e.n_min;
     if (rank < nq) {
-      double* Xq = q == 0 ? K.X[0] : K.X[1];
-      double* Yq = q == 0 ? K.Y[0] : K.Y[1];
+      real* Xq = q == 0 ? K.X[0] : K.X[1];
+      real* Yq = q == 0 ? K.Y[0] : K.Y[1];
       Xq[NB + rank] = T(ii);
       Yq[NB + rank] = v;
       bad |= q == 0 ? (v < 0.0) : (v > 0.0);
@@ -788,8 +810,8 @@ __device__ __forceinline__ bool fill_true_knots(const SmemLayout& L, const Knots
       if (!(((bm | bn) >> lane) & 1u)) continue;
       int i = (c << 5) + lane;
       int ii = i;
-      double v = imf[i];
-      double dp = v - imf[i - 1], dn = imf[i + 1] - v;
+      real v = imf[i];
+      real dp = v - imf[i - 1], dn = imf[i + 1] - v;
       if (!(dp * dn < 0.0)) {       // plateau extremum: report the run's midpoint
         int j = i;
         while (j + 1 < N && imf[j + 1] == v) ++j;
@@ -823,7 +845,7 @@ __device__ __forceinline__ int ind_of(const Ctl& C, int q, int n, int NB, int k)
 __device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K, const ExtInfo& e,
                                             int N, int NB, const TimeAxis& T, int lane) {
   Ctl& C = *L.ctl;
-  const double* S = L.imf;
+  const real* S = L.imf;
   const int nM = e.n_max, nm = e.n_min;
   if (lane == 0) {
     int* l0 = C.mlist[0];
@@ -890,9 +912,12 @@ __device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K,
     if (c2 == 0) r0[c2++] = imL;
     if (c3 == 0) r1[c3++] = inL;
     // ---- mirrored point does not reach the boundary (kernels.py:469-503) ----
-    const double T0 = T(0), TN = T(N - 1);
-    double tl = T(lsym);
-    if (2.0 * tl - T(l1[0]) > T0 || 2.0 * tl - T(l0[0]) > T0) {
+    const real T0 = T(0), TN = T(N - 1);
+    real tl = T(lsym);
+    // the mirrored positions are stored as REAL_T before the compares
+    // (kernels.py:471-472, 488-489): in the FP32 build that rounds them
+    const real tl1 = 2.0 * tl - T(l1[0]), tl0 = 2.0 * tl - T(l0[0]);
+    if (tl1 > T0 || tl0 > T0) {
       if (lsym == im0) {
         c0 = 0;
         for (int k = min(nM, NB) - 1; k >= 0; --k) l0[c0++] = ind_of(C, 0, nM, NB, k);
@@ -902,8 +927,9 @@ __device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K,
       }
       lsym = 0;
     }
-    double tr = T(rsym);
-    if (2.0 * tr - T(r1[c3 - 1]) < TN || 2.0 * tr - T(r0[c2 - 1]) < TN) {
+    real tr = T(rsym);
+    const real tr1 = 2.0 * tr - T(r1[c3 - 1]), tr0 = 2.0 * tr - T(r0[c2 - 1]);
+    if (tr1 < TN || tr0 < TN) {
       if (rsym == imL) {
         c2 = 0;
         for (int k = nM - 1; k >= max(nM - NB, 0); --k) r0[c2++] = ind_of(C, 0, nM, NB, k);
@@ -931,8 +957,8 @@ __device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K,
     int idx = C.mlist[q][j];
     int side = q & 1;
     bool left = q < 2;
-    double pos = 2.0 * T(left ? C.lsym : C.rsym) - T(idx);
-    double val = S[idx];
+    real pos = 2.0 * T(left ? C.lsym : C.rsym) - T(idx);
+    real val = S[idx];
     int nside = side == 0 ? nM : nm;
     int slot = left ? (NB - cq + j) : (NB + nside + j);
     (side == 0 ? K.X[0] : K.X[1])[slot] = pos;
@@ -951,33 +977,33 @@ __device__ __forceinline__ bool mirror_both(const SmemLayout& L, const Knots& K,
 // outside the table (or not positive integers, as unsorted knot lists can
 // give) take the divisions.
 template <bool kInt = false>
-__device__ __forceinline__ void setup_row(const double* x, const double* y, int n, int k, int m,
-                                          double& a, double& b, double& c, double& d) {
+__device__ __forceinline__ void setup_row(const real* x, const real* y, int n, int k, int m,
+                                          real& a, real& b, real& c, real& d) {
   if (k == 0) {
-    double h0 = x[1] - x[0], h1 = x[2] - x[1];
-    double rhs1 = 6.0 * ((y[2] - y[1]) / h1 - (y[1] - y[0]) / h0);
+    real h0 = x[1] - x[0], h1 = x[2] - x[1];
+    real rhs1 = 6.0 * ((y[2] - y[1]) / h1 - (y[1] - y[0]) / h0);
     a = 0.0; b = h0 + 2.0 * h1; c = h1 - h0; d = h1 * rhs1 / (h0 + h1);
   } else if (k == m - 1) {
-    double hnm3 = x[n - 2] - x[n - 3], hnm2 = x[n - 1] - x[n - 2];
-    double rhs = 6.0 * ((y[n - 1] - y[n - 2]) / hnm2 - (y[n - 2] - y[n - 3]) / hnm3);
+    real hnm3 = x[n - 2] - x[n - 3], hnm2 = x[n - 1] - x[n - 2];
+    real rhs = 6.0 * ((y[n - 1] - y[n - 2]) / hnm2 - (y[n - 2] - y[n - 3]) / hnm3);
     a = hnm3 - hnm2; b = 2.0 * hnm3 + hnm2; c = 0.0; d = hnm3 * rhs / (hnm3 + hnm2);
   } else {
     int i = k + 1;
-    double h_im1 = x[i] - x[i - 1], h_i = x[i + 1] - x[i];
+    real h_im1 = x[i] - x[i - 1], h_i = x[i + 1] - x[i];
     a = h_im1; b = 2.0 * (h_im1 + h_i); c = h_i;
 #if EMDB_SETUP_NB
     bool slow = false;
-    const double sr = div_nb(y[i + 1] - y[i], h_i, slow);
-    const double sl = div_nb(y[i] - y[i - 1], h_im1, slow);
+    const real sr = div_nb(y[i + 1] - y[i], h_i, slow);
+    const real sl = div_nb(y[i] - y[i - 1], h_im1, slow);
     d = slow ? 6.0 * ((y[i + 1] - y[i]) / h_i - (y[i] - y[i - 1]) / h_im1) : 6.0 * (sr - sl);
 #else
     if (kInt) {
-      const bool ok = h_i >= 1.0 && h_i <= (double)kRcpTab && h_im1 >= 1.0 &&
-                      h_im1 <= (double)kRcpTab;
+      const bool ok = h_i >= 1.0 && h_i <= (real)kRcpTab && h_im1 >= 1.0 &&
+                      h_im1 <= (real)kRcpTab;
       const int ji = ok ? (int)h_i : 1, jm = ok ? (int)h_im1 : 1;
-      bool slow = !ok || (double)ji != h_i || (double)jm != h_im1;
-      const double sr = div_q(y[i + 1] - y[i], h_i, g_rcp.v[ji], slow);
-      const double sl = div_q(y[i] - y[i - 1], h_im1, g_rcp.v[jm], slow);
+      bool slow = !ok || (real)ji != h_i || (real)jm != h_im1;
+      const real sr = div_q(y[i + 1] - y[i], h_i, g_rcp.v[ji], slow);
+      const real sl = div_q(y[i] - y[i - 1], h_im1, g_rcp.v[jm], slow);
       d = slow ? 6.0 * (EMDB_DIV_RARE(y[i + 1] - y[i], h_i) - EMDB_DIV_RARE(y[i] - y[i - 1], h_im1))
                : 6.0 * (sr - sl);
     } else {
@@ -987,33 +1013,33 @@ __device__ __forceinline__ void setup_row(const double* x, const double* y, int 
   }
 }
 
-__device__ __forceinline__ void pcr_row(const double* __restrict__ Pa, double* __restrict__ Pn,
+__device__ __forceinline__ void pcr_row(const real* __restrict__ Pa, real* __restrict__ Pn,
                                         int cap, int r, int k, int s, int mq) {
   const bool hl = k - s >= 0, hr = k + s < mq;
   const int rl = r - s, rr = r + s;
-  const double ak = Pa[r], bk = Pa[cap + r], ck = Pa[2 * cap + r], dk = Pa[3 * cap + r];
-  const double b_left = hl ? Pa[cap + rl] : 1.0;
-  const double b_right = hr ? Pa[cap + rr] : 1.0;
+  const real ak = Pa[r], bk = Pa[cap + r], ck = Pa[2 * cap + r], dk = Pa[3 * cap + r];
+  const real b_left = hl ? Pa[cap + rl] : 1.0;
+  const real b_right = hr ? Pa[cap + rr] : 1.0;
 #if EMDB_PCR_NB
   bool sl = false, sr = false;
-  const double ql = div_nb(ak, b_left, sl);
-  const double qr = div_nb(ck, b_right, sr);
-  double alpha = hl ? ql : 0.0;
-  double beta = hr ? qr : 0.0;
+  const real ql = div_nb(ak, b_left, sl);
+  const real qr = div_nb(ck, b_right, sr);
+  real alpha = hl ? ql : 0.0;
+  real beta = hr ? qr : 0.0;
   if ((hl && sl) || (hr && sr)) {
     alpha = hl ? EMDB_DIV_RARE(ak, b_left) : 0.0;
     beta = hr ? EMDB_DIV_RARE(ck, b_right) : 0.0;
   }
 #else
-  const double alpha = hl ? ak / b_left : 0.0;
-  const double beta = hr ? ck / b_right : 0.0;
+  const real alpha = hl ? ak / b_left : 0.0;
+  const real beta = hr ? ck / b_right : 0.0;
 #endif
-  const double a_left = hl ? Pa[rl] : 0.0;
-  const double c_left = hl ? Pa[2 * cap + rl] : 0.0;
-  const double d_left = hl ? Pa[3 * cap + rl] : 0.0;
-  const double a_right = hr ? Pa[rr] : 0.0;
-  const double c_right = hr ? Pa[2 * cap + rr] : 0.0;
-  const double d_right = hr ? Pa[3 * cap + rr] : 0.0;
+  const real a_left = hl ? Pa[rl] : 0.0;
+  const real c_left = hl ? Pa[2 * cap + rl] : 0.0;
+  const real d_left = hl ? Pa[3 * cap + rl] : 0.0;
+  const real a_right = hr ? Pa[rr] : 0.0;
+  const real c_right = hr ? Pa[2 * cap + rr] : 0.0;
+  const real d_right = hr ? Pa[3 * cap + rr] : 0.0;
   Pn[r] = -alpha * a_left;
   Pn[2 * cap + r] = -beta * c_right;
   Pn[cap + r] = bk - alpha * c_left - beta * a_right;
@@ -1027,18 +1053,18 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
   const int m1 = kcnt1 >= 4 ? kcnt1 - 2 : 0;
   const int mt = m0 + m1;
   const int cap = K.cap;
-  const double* x0b = K.X[0] + kbase0;
-  const double* x1b = K.X[1] + kbase1;
-  const double* y0b = K.Y[0] + kbase0;
-  const double* y1b = K.Y[1] + kbase1;
+  const real* x0b = K.X[0] + kbase0;
+  const real* x1b = K.X[1] + kbase1;
+  const real* y0b = K.Y[0] + kbase0;
+  const real* y1b = K.Y[1] + kbase1;
   for (int r = tid; r < mt; r += NT) {
     const bool s0 = r < m0;
     const int k = s0 ? r : r - m0;
-    const double* x = s0 ? x0b : x1b;
-    const double* y = s0 ? y0b : y1b;
-    double a, b, c, d;
+    const real* x = s0 ? x0b : x1b;
+    const real* y = s0 ? y0b : y1b;
+    real a, b, c, d;
     setup_row<kInt>(x, y, s0 ? kcnt0 : kcnt1, k, s0 ? m0 : m1, a, b, c, d);
-    double* P = K.P[0];
+    real* P = K.P[0];
     P[r] = a; P[cap + r] = b; P[2 * cap + r] = c; P[3 * cap + r] = d;
   }
   __syncthreads();
@@ -1047,8 +1073,8 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
   int cur = 0;
   int fin0 = 0, fin1 = 0;
   for (int s = 1; s < mmax; s *= 2) {
-    const double* __restrict__ Pa = cur ? K.P[1] : K.P[0];
-    double* __restrict__ Pn = cur ? K.P[0] : K.P[1];
+    const real* __restrict__ Pa = cur ? K.P[1] : K.P[0];
+    real* __restrict__ Pn = cur ? K.P[0] : K.P[1];
     // two rows per trip: independent division chains overlap
     constexpr int kPair = NT > kThreads ? EMDB_WIDE_PCR_PAIR : EMDB_PCR_PAIR;
     for (int r = tid; r < mt; r += (1 + kPair) * NT) {
@@ -1080,24 +1106,24 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
     const int k = s0 ? r : r - m0;
     const int mq = s0 ? m0 : m1;
     const int n = s0 ? kcnt0 : kcnt1;
-    const double* Pf = (s0 ? fin0 : fin1) ? K.P[1] : K.P[0];
-    double* M = s0 ? K.M[0] : K.M[1];
-    const double* x = s0 ? x0b : x1b;
-    double Mk1 = Pf[3 * cap + r] / Pf[cap + r];
+    const real* Pf = (s0 ? fin0 : fin1) ? K.P[1] : K.P[0];
+    real* M = s0 ? K.M[0] : K.M[1];
+    const real* x = s0 ? x0b : x1b;
+    real Mk1 = Pf[3 * cap + r] / Pf[cap + r];
     M[k + 1] = Mk1;
 #if EMDB_FAST_DIV == 1
-    double* R = s0 ? K.R[0] : K.R[1];
+    real* R = s0 ? K.R[0] : K.R[1];
     R[k] = 1.0 / (x[k + 1] - x[k]);
     if (k == mq - 1) R[k + 1] = 1.0 / (x[k + 2] - x[k + 1]);
 #endif
     if (k == 0) {
-      double M2 = Pf[3 * cap + r + 1] / Pf[cap + r + 1];
-      double h0 = x[1] - x[0], h1 = x[2] - x[1];
+      real M2 = Pf[3 * cap + r + 1] / Pf[cap + r + 1];
+      real h0 = x[1] - x[0], h1 = x[2] - x[1];
       M[0] = ((h0 + h1) * Mk1 - h0 * M2) / h1;
     }
     if (k == mq - 1) {
-      double Mnm3 = Pf[3 * cap + r - 1] / Pf[cap + r - 1];
-      double hnm3 = x[n - 2] - x[n - 3], hnm2 = x[n - 1] - x[n - 2];
+      real Mnm3 = Pf[3 * cap + r - 1] / Pf[cap + r - 1];
+      real hnm3 = x[n - 2] - x[n - 3], hnm2 = x[n - 1] - x[n - 2];
       M[n - 1] = ((hnm3 + hnm2) * Mk1 - hnm2 * Mnm3) / hnm3;
     }
   }
@@ -1107,66 +1133,68 @@ __device__ __forceinline__ void solve_splines(const Knots& K, int kbase0, int kb
 
 // One PCR row update (kernels.py:651-668), in the reference's operation order.
 struct SideView {
-  const double* x;
-  const double* y;
-  const double* M;
-  const double* R;
+  const real* x;
+  const real* y;
+  const real* M;
+  const real* R;
   int n;          // knots
   int nl, nt;     // mirrored-left and true knots
 };
 
 // Envelope value at t in knot segment lo (kernels.py:706-733).
-__device__ __forceinline__ double eval_seg(const SideView& s, double t, int lo) {
-  const double* x = s.x;
-  const double* y = s.y;
+__device__ __forceinline__ real eval_seg(const SideView& s, real t, int lo) {
+  const real* x = s.x;
+  const real* y = s.y;
   if (s.n == 2) {
-    double slope = (y[1] - y[0]) / (x[1] - x[0]);
+    real slope = (y[1] - y[0]) / (x[1] - x[0]);
     return y[0] + slope * (t - x[0]);
   }
   if (s.n == 3) {
-    double l0 = (t - x[1]) * (t - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
-    double l1 = (t - x[0]) * (t - x[2]) / ((x[1] - x[0]) * (x[1] - x[2]));
-    double l2 = (t - x[0]) * (t - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
+    real l0 = (t - x[1]) * (t - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
+    real l1 = (t - x[0]) * (t - x[2]) / ((x[1] - x[0]) * (x[1] - x[2]));
+    real l2 = (t - x[0]) * (t - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
     return y[0] * l0 + y[1] * l1 + y[2] * l2;
   }
-  double x0 = x[lo], x1 = x[lo + 1];
-  double y0 = y[lo], y1 = y[lo + 1];
-  double M0 = s.M[lo], M1 = s.M[lo + 1];
-  double h = x1 - x0;
-  double A = (x1 - t) / h;
-  double B = (t - x0) / h;
+  real x0 = x[lo], x1 = x[lo + 1];
+  real y0 = y[lo], y1 = y[lo + 1];
+  real M0 = s.M[lo], M1 = s.M[lo + 1];
+  real h = x1 - x0;
+  real A = (x1 - t) / h;
+  real B = (t - x0) / h;
   return A * y0 + B * y1 + ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h) / 6.0;
 }
 
 // eval_seg with the quotients taken from reciprocals (EMDB_FAST_DIV 1..3), in
 // the same operation order; sets `slow` when a quotient needs the division,
 // and the caller then re-evaluates the sample with eval_seg.
-__device__ __forceinline__ double eval_seg_q(const SideView& s, double t, int lo, bool& slow) {
+#if !EMDB_F32
+__device__ __forceinline__ real eval_seg_q(const SideView& s, real t, int lo, bool& slow) {
   if (s.n < 4) return EMDB_EVAL_RARE(s, t, lo);
-  const double* x = s.x;
-  const double* y = s.y;
-  double x0 = x[lo], x1 = x[lo + 1];
-  double y0 = y[lo], y1 = y[lo + 1];
-  double M0 = s.M[lo], M1 = s.M[lo + 1];
-  double h = x1 - x0;
+  const real* x = s.x;
+  const real* y = s.y;
+  real x0 = x[lo], x1 = x[lo + 1];
+  real y0 = y[lo], y1 = y[lo + 1];
+  real M0 = s.M[lo], M1 = s.M[lo + 1];
+  real h = x1 - x0;
 #if EMDB_FAST_DIV == 2
-  double A = (x1 - t) / h;
-  double B = (t - x0) / h;
+  real A = (x1 - t) / h;
+  real B = (t - x0) / h;
 #else
 #if EMDB_FAST_DIV == 1
-  double rh = s.R[lo];
+  real rh = s.R[lo];
 #else
-  double rh = 1.0 / h;
+  real rh = 1.0 / h;
 #endif
-  double A = div_q(x1 - t, h, rh, slow);
-  double B = div_q(t - x0, h, rh, slow);
+  real A = div_q(x1 - t, h, rh, slow);
+  real B = div_q(t - x0, h, rh, slow);
 #endif
-  double num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
+  real num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
   return (A * y0 + B * y1) + div_q(num, 6.0, kInv6, slow);
 }
+#endif
 
 // The reference's per-sample binary search (kernels.py:722-726).
-__device__ __forceinline__ int search_seg(const SideView& s, double t) {
+__device__ __forceinline__ int search_seg(const SideView& s, real t) {
   int lo = 0, hi = s.n - 2;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
@@ -1176,13 +1204,13 @@ __device__ __forceinline__ int search_seg(const SideView& s, double t) {
 }
 
 // Out-of-line bodies of the rare paths declared with div_slow.
-__device__ __noinline__ double eval_seg_cold(const double* x, const double* y, const double* M,
-                                             int n, double t, int lo) {
+__device__ __noinline__ real eval_seg_cold(const real* x, const real* y, const real* M,
+                                             int n, real t, int lo) {
   SideView s;
   s.x = x; s.y = y; s.M = M; s.R = nullptr; s.n = n; s.nl = 0; s.nt = 0;
   return eval_seg(s, t, lo);
 }
-__device__ __noinline__ int search_seg_cold(const double* x, int n, double t) {
+__device__ __noinline__ int search_seg_cold(const real* x, int n, real t) {
   SideView s;
   s.x = x; s.y = nullptr; s.M = nullptr; s.R = nullptr; s.n = n; s.nl = 0; s.nt = 0;
   return search_seg(s, t);
@@ -1190,15 +1218,15 @@ __device__ __noinline__ int search_seg_cold(const double* x, int n, double t) {
 
 // 128-lane tree of the reference (kernels.py:794-804), on warp 0, for a value
 // each thread has stored at red[q*128 + tid].  op 0: sum, 1: fmax, 2: fmin.
-__device__ __forceinline__ double lane_tree(const double* red, int lane, int op) {
-  double v0 = red[lane], v1 = red[lane + 32], v2 = red[lane + 64], v3 = red[lane + 96];
-  double r;
+__device__ __forceinline__ real lane_tree(const real* red, int lane, int op) {
+  real v0 = red[lane], v1 = red[lane + 32], v2 = red[lane + 64], v3 = red[lane + 96];
+  real r;
   if (op == 0) r = (v0 + v2) + (v1 + v3);
   else if (op == 1) r = fmax(fmax(v0, v2), fmax(v1, v3));
   else r = fmin(fmin(v0, v2), fmin(v1, v3));
 #pragma unroll
   for (int s = 16; s > 0; s >>= 1) {
-    double o = __shfl_down_sync(kFull, r, s);
+    real o = __shfl_down_sync(kFull, r, s);
     if (op == 0) r = r + o;
     else if (op == 1) r = fmax(r, o);
     else r = fmin(r, o);
@@ -1207,22 +1235,22 @@ __device__ __forceinline__ double lane_tree(const double* red, int lane, int op)
 }
 
 struct PassSums {
-  double sq, dsq, osq, std_, omax, omin;
+  real sq, dsq, osq, std_, omax, omin;
   bool bad;
   bool oor;
 };
 
-__device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) {
-  double diff = nw - old;
+__device__ __forceinline__ void accumulate(PassSums& ps, real old, real nw) {
+  real diff = nw - old;
   ps.sq += nw * nw;
   ps.dsq += diff * diff;
   ps.osq += old * old;
 #if EMDB_ACC_NB
   bool slow = false;
-  double qd = div_nb(diff, nw, slow);
+  real qd = div_nb(diff, nw, slow);
   if (slow) qd = diff / nw;
 #else
-  double qd = diff / nw;
+  real qd = diff / nw;
 #endif
   ps.std_ += qd * qd;
   ps.omax = fmax(ps.omax, old);
@@ -1237,43 +1265,43 @@ __device__ __forceinline__ void accumulate(PassSums& ps, double old, double nw) 
 // Σold², max, min | Σquotient²; 256 threads: the first two | the rest --
 // and write the lanes' partials to red[128 * sum + l] for the trees.
 template <int NT>
-__device__ __forceinline__ void wide_lane_sums(double* red, const double* __restrict__ oldv,
-                                               const double* imf, const double* __restrict__ qbuf,
+__device__ __forceinline__ void wide_lane_sums(real* red, const real* __restrict__ oldv,
+                                               const real* imf, const real* __restrict__ qbuf,
                                                int N, int tid) {
   constexpr int NG = NT / kThreads;
   static_assert(NG == 2 || NG == 4, "wide instances have 256 or 512 threads");
   const int g = tid / kThreads, l = tid % kThreads;
   if (g == 0) {
-    double s = 0.0, s2 = 0.0;
+    real s = 0.0, s2 = 0.0;
 #pragma unroll kLaneUnroll
     for (int i = l; i < N; i += kThreads) {
-      const double nw = imf[i];
+      const real nw = imf[i];
       s += nw * nw;
       if (NG == 2) {
-        const double diff = nw - oldv[i];
+        const real diff = nw - oldv[i];
         s2 += diff * diff;
       }
     }
     red[l] = s;
     if (NG == 2) red[128 + l] = s2;
   } else if (NG == 4 && g == 1) {
-    double s = 0.0;
+    real s = 0.0;
 #pragma unroll kLaneUnroll
     for (int i = l; i < N; i += kThreads) {
-      const double diff = imf[i] - oldv[i];
+      const real diff = imf[i] - oldv[i];
       s += diff * diff;
     }
     red[128 + l] = s;
   } else if (g == NG / 2) {
-    double s = 0.0, mx = -1e30, mn = 1e30, sq = 0.0;
+    real s = 0.0, mx = -1e30, mn = 1e30, sq = 0.0;
 #pragma unroll kLaneUnroll
     for (int i = l; i < N; i += kThreads) {
-      const double old = oldv[i];
+      const real old = oldv[i];
       s += old * old;
       mx = fmax(mx, old);
       mn = fmin(mn, old);
       if (NG == 2) {
-        const double q = qbuf[i];
+        const real q = qbuf[i];
         sq += q * q;
       }
     }
@@ -1282,10 +1310,10 @@ __device__ __forceinline__ void wide_lane_sums(double* red, const double* __rest
     red[640 + l] = mn;
     if (NG == 2) red[384 + l] = sq;
   } else if (NG == 4 && g == 3) {
-    double s = 0.0;
+    real s = 0.0;
 #pragma unroll kLaneUnroll
     for (int i = l; i < N; i += kThreads) {
-      const double q = qbuf[i];
+      const real q = qbuf[i];
       s += q * q;
     }
     red[384 + l] = s;
@@ -1299,36 +1327,38 @@ __device__ __forceinline__ void wide_lane_sums(double* red, const double* __rest
 // exhaustively for every pair with h <= 65536 (2.1e9 pairs).  Anything outside
 // (h beyond the table, a not in [0, h]) sets `slow`, and the caller redoes the
 // sample with eval_seg.  Same operation order as eval_seg otherwise.
-__device__ __forceinline__ double eval_seg_int(const SideView& s, double t, int lo, bool& slow,
+#if !EMDB_F32
+__device__ __forceinline__ real eval_seg_int(const SideView& s, real t, int lo, bool& slow,
                                                bool sorted = false) {
   if (s.n < 4) return EMDB_EVAL_RARE(s, t, lo);
-  const double* x = s.x;
-  const double* y = s.y;
-  double x0 = x[lo], x1 = x[lo + 1];
-  double y0 = y[lo], y1 = y[lo + 1];
-  double M0 = s.M[lo], M1 = s.M[lo + 1];
-  double h = x1 - x0;
-  const double a = x1 - t, b = t - x0;
+  const real* x = s.x;
+  const real* y = s.y;
+  real x0 = x[lo], x1 = x[lo + 1];
+  real y0 = y[lo], y1 = y[lo + 1];
+  real M0 = s.M[lo], M1 = s.M[lo + 1];
+  real h = x1 - x0;
+  const real a = x1 - t, b = t - x0;
   int hi;
   if (EMDB_SORTED_NOCHECK && sorted) {
     // strictly increasing integer knots and the segment that holds t: h is an
     // integer >= 1 and a, b lie in [0, h]; only the table bound is left
-    const bool in = h <= (double)kRcpTab;
+    const bool in = h <= (real)kRcpTab;
     hi = in ? (int)h : 1;
     slow |= !in;
   } else {
-    const bool in = h >= 1.0 && h <= (double)kRcpTab && a >= 0.0 && b >= 0.0 && a <= h && b <= h;
+    const bool in = h >= 1.0 && h <= (real)kRcpTab && a >= 0.0 && b >= 0.0 && a <= h && b <= h;
     hi = in ? (int)h : 1;
-    slow |= !in || (double)hi != h;
+    slow |= !in || (real)hi != h;
   }
-  const double r = g_rcp.v[hi];
-  double A = a * r;
+  const real r = g_rcp.v[hi];
+  real A = a * r;
   A = fma(fma(-A, h, a), r, A);
-  double B = b * r;
+  real B = b * r;
   B = fma(fma(-B, h, b), r, B);
-  double num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
+  real num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
   return (A * y0 + B * y1) + div_q(num, 6.0, kInv6, slow);
 }
+#endif
 
 // One sift pass after the extrema scan of the current proto-IMF: knots,
 // mirroring, both splines, then the fused envelope / mean / update / partial
@@ -1345,7 +1375,7 @@ template <int NT, int kGroup, bool kInt>
 __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
                                               int N, int NB, const TimeAxis& T, int tid, int warp,
                                               int lane, int place = kPlaceSmem,
-                                              double* park_old = nullptr, double* qbuf = nullptr) {
+                                              real* park_old = nullptr, real* qbuf = nullptr) {
   constexpr bool kWide = NT > kThreads;
   // kGroup >= 0: one placement, fixed at compile time.  kGroup == kOnChip /
   // kOffChip: one instance for the on-chip (shared, borrow) or off-chip
@@ -1357,7 +1387,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
                                            : place == kPlacePark ? kPlacePark : kPlaceSlab)
                                         : place;
   Ctl& C = *L.ctl;
-  double* imf = L.imf;
+  real* imf = L.imf;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
   Knots K = kPlace == kPlaceSmem    ? place_knots(L.arena, kc0, kc1)
            : kPlace == kPlaceSplit  ? place_knots_split(L.arena, L.arena_bytes, slab, kc0, kc1)
@@ -1383,7 +1413,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     for (int i = tid - 32; i < N; i += NT - 32) park_old[i] = imf[i];
   } else if (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark) {
     // park the proto-IMF while warp 0 mirrors; the PCR buffers overwrite it
-    double* save = borrow_save(slab);
+    real* save = borrow_save(slab);
     for (int i = tid - 32; i < N; i += kThreads - 32) save[i] = imf[i];
   }
   ps.bad = __syncthreads_or(bad || mbad) != 0;
@@ -1391,7 +1421,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   const int kb0 = C.kbase[0], kb1 = C.kbase[1], kn0 = C.kcnt[0], kn1 = C.kcnt[1];
   solve_splines<NT, kInt && EMDB_SETUP_TAB>(K, kb0, kb1, kn0, kn1, tid,
                                              EMDB_LOAD_CLOCKS ? &C : nullptr);
-  const double* oldv = kWide ? park_old
+  const real* oldv = kWide ? park_old
                      : (kPlace == kPlaceBorrow || kPlace == kPlaceBorrow2 || kPlace == kPlacePark)
                             ? borrow_save(slab) : imf;
 
@@ -1413,16 +1443,16 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   const int nch = (N + 31) >> 5;
   // chunk c = (tid>>5) + 4j is scanned by warp wc(c); its rank offset is woff[wc] + pre[c]
   // mirrored knots of both envelopes, for the O(1) segment count (nbsym <= 2)
-  constexpr double kInf = __builtin_huge_val();
-  const double l00 = sv0.nl > 0 ? sv0.x[0] : kInf, l01 = sv0.nl > 1 ? sv0.x[1] : kInf;
-  const double l10 = sv1.nl > 0 ? sv1.x[0] : kInf, l11 = sv1.nl > 1 ? sv1.x[1] : kInf;
+  constexpr real kInf = __builtin_huge_val();
+  const real l00 = sv0.nl > 0 ? sv0.x[0] : kInf, l01 = sv0.nl > 1 ? sv0.x[1] : kInf;
+  const real l10 = sv1.nl > 0 ? sv1.x[0] : kInf, l11 = sv1.nl > 1 ? sv1.x[1] : kInf;
   const int nr0 = sv0.n - sv0.nl - sv0.nt, nr1 = sv1.n - sv1.nl - sv1.nt;
-  const double r00 = nr0 > 0 ? sv0.x[sv0.nl + sv0.nt] : kInf, r01 = nr0 > 1 ? sv0.x[sv0.nl + sv0.nt + 1] : kInf;
-  const double r10 = nr1 > 0 ? sv1.x[sv1.nl + sv1.nt] : kInf, r11 = nr1 > 1 ? sv1.x[sv1.nl + sv1.nt + 1] : kInf;
+  const real r00 = nr0 > 0 ? sv0.x[sv0.nl + sv0.nt] : kInf, r01 = nr0 > 1 ? sv0.x[sv0.nl + sv0.nt + 1] : kInf;
+  const real r10 = nr1 > 0 ? sv1.x[sv1.nl + sv1.nt] : kInf, r11 = nr1 > 1 ? sv1.x[sv1.nl + sv1.nt + 1] : kInf;
   (void)nch;
   const unsigned incl = lane == 31 ? kFull : ((2u << lane) - 1u);
   // knot segment of sample i for both envelopes
-  auto segs = [&](int i, double t, int& lo0, int& lo1) {
+  auto segs = [&](int i, real t, int& lo0, int& lo1) {
     lo0 = 0;
     lo1 = 0;
     if (fast) {
@@ -1443,7 +1473,7 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   // T is strictly increasing, so the knot spans cover every sample iff they
   // cover the first and the last one
   if (N > 0) {
-    const double t0 = T(0), tN = T(N - 1);
+    const real t0 = T(0), tN = T(N - 1);
     oor = (t0 < sv0.x[0]) || (tN > sv0.x[sv0.n - 1]) || (t0 < sv1.x[0]) || (tN > sv1.x[sv1.n - 1]);
   }
   // two samples per trip (i, i+NT): independent evaluation chains overlap;
@@ -1451,14 +1481,14 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   for (int i = tid; i < N; i += (1 + EMDB_EVAL_PAIR) * NT) {
     const int i2 = i + NT;
     const bool has2 = EMDB_EVAL_PAIR && i2 < N;
-    const double t = T(i);
-    const double t2 = has2 ? T(i2) : t;
+    const real t = T(i);
+    const real t2 = has2 ? T(i2) : t;
     int lo0, lo1, lo0b, lo1b;
     segs(i, t, lo0, lo1);
     if (has2) segs(i2, t2, lo0b, lo1b); else { lo0b = lo0; lo1b = lo1; }
 #if EMDB_FAST_DIV
     bool slow = false;
-    double emax, emin, emax2 = 0.0, emin2 = 0.0;
+    real emax, emin, emax2 = 0.0, emin2 = 0.0;
     if (kInt) {
       emax = eval_seg_int(sv0, t, lo0, slow, fast);
       emin = eval_seg_int(sv1, t, lo1, slow, fast);
@@ -1481,36 +1511,37 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
       emin2 = EMDB_EVAL_RARE(sv1, t2, lo1b);
     }
 #else
-    const double emax = eval_seg(sv0, t, lo0);
-    const double emin = eval_seg(sv1, t, lo1);
-    const double emax2 = eval_seg(sv0, t2, lo0b);
-    const double emin2 = eval_seg(sv1, t2, lo1b);
+    const real emax = eval_seg(sv0, t, lo0);
+    const real emin = eval_seg(sv1, t, lo1);
+    const real emax2 = eval_seg(sv0, t2, lo0b);
+    const real emin2 = eval_seg(sv1, t2, lo1b);
 #endif
     if (kWide) {
       // the update, and accumulate()'s quotient from the same operands
-      const double old = oldv[i];
-      const double nw = old - 0.5 * (emax + emin);
+      const real old = oldv[i];
+      const real mean = 0.5 * (emax + emin);
+      const real nw = old - mean;
       imf[i] = nw;
       qbuf[i] = (nw - old) / nw;
       continue;
     }
     {
-      const double mean = 0.5 * (emax + emin);
-      const double old = oldv[i];
-      const double nw = old - mean;
+      const real mean = 0.5 * (emax + emin);
+      const real old = oldv[i];
+      const real nw = old - mean;
       imf[i] = nw;
       accumulate(ps, old, nw);
     }
     if (has2) {
-      const double mean = 0.5 * (emax2 + emin2);
-      const double old = oldv[i2];
-      const double nw = old - mean;
+      const real mean = 0.5 * (emax2 + emin2);
+      const real old = oldv[i2];
+      const real nw = old - mean;
       imf[i2] = nw;
       accumulate(ps, old, nw);
     }
   }
   // per-lane partial sums, then the reference's 128-lane trees on warp 0
-  double* red = kPlace == kPlaceSlab ? L.red : K.red;
+  real* red = kPlace == kPlaceSlab ? L.red : K.red;
   if constexpr (kWide && !EMDB_WIDE_OVERLAP) {
     __syncthreads();
     EMDB_PH(&C, 5);
@@ -1523,8 +1554,8 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
     EMDB_PH(&C, 5);
     if (tid < kThreads) {
       for (int i = tid; i < N; i += kThreads) {
-        const double old = oldv[i], nw = imf[i], qd = qbuf[i];
-        const double diff = nw - old;
+        const real old = oldv[i], nw = imf[i], qd = qbuf[i];
+        const real diff = nw - old;
         ps.sq += nw * nw;
         ps.dsq += diff * diff;
         ps.osq += old * old;
@@ -1547,10 +1578,10 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   // the six trees spread over the warps (warp w: sum w; warps 0/1 also the
   // max / min tree); the next extrema scan's barrier publishes C.sums
   if (!kWide || warp < kWarps) {
-    const double a = lane_tree(red + 128 * warp, lane, 0);
+    const real a = lane_tree(red + 128 * warp, lane, 0);
     if (lane == 0) C.sums[warp] = a;
     if (warp < 2) {
-      const double b = lane_tree(red + 128 * (4 + warp), lane, 1 + warp);
+      const real b = lane_tree(red + 128 * (4 + warp), lane, 1 + warp);
       if (lane == 0) C.sums[4 + warp] = b;
     }
   }
@@ -1558,12 +1589,12 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
   if (kWide && EMDB_WIDE_OVERLAP) __syncthreads();
 #else
   if (warp == 0) {
-    double a0 = lane_tree(red, lane, 0);
-    double a1 = lane_tree(red + 128, lane, 0);
-    double a2 = lane_tree(red + 256, lane, 0);
-    double a3 = lane_tree(red + 384, lane, 0);
-    double a4 = lane_tree(red + 512, lane, 1);
-    double a5 = lane_tree(red + 640, lane, 2);
+    real a0 = lane_tree(red, lane, 0);
+    real a1 = lane_tree(red + 128, lane, 0);
+    real a2 = lane_tree(red + 256, lane, 0);
+    real a3 = lane_tree(red + 384, lane, 0);
+    real a4 = lane_tree(red + 512, lane, 1);
+    real a5 = lane_tree(red + 640, lane, 2);
     if (lane == 0) {
       C.sums[0] = a0; C.sums[1] = a1; C.sums[2] = a2;
       C.sums[3] = a3; C.sums[4] = a4; C.sums[5] = a5;
@@ -1618,9 +1649,9 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
   char* slab = p.slab + (size_t)blockIdx.x * p.slab_stride;
   // wide instance: the parked proto-IMF and the stop-test quotients (and the
   // proto-IMF itself for kGImf), past the knot slab in this CTA's stride
-  double* park_old = kWide ? reinterpret_cast<double*>(slab + p.park_off) : nullptr;
-  double* qbuf = kWide ? reinterpret_cast<double*>(slab + p.q_off) : nullptr;
-  double* gimf = kGImf ? reinterpret_cast<double*>(slab + p.imf_off) : nullptr;
+  real* park_old = kWide ? reinterpret_cast<real*>(slab + p.park_off) : nullptr;
+  real* qbuf = kWide ? reinterpret_cast<real*>(slab + p.q_off) : nullptr;
+  real* gimf = kGImf ? reinterpret_cast<real*>(slab + p.imf_off) : nullptr;
 
   for (;;) {
     if (tid == 0) Cs->job = atomicAdd(p.queue, 1);
@@ -1630,15 +1661,15 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     const int b = p.order ? p.order[job] : job;
     const int64_t off = p.offsets ? p.offsets[b] : (int64_t)b * p.dense_n;
     const int N = p.offsets ? (int)(p.offsets[b + 1] - off) : p.dense_n;
-    const double* S = p.values + off;
-    double* out = p.imfs + (int64_t)MAXI * off;
+    const real* S = p.values + off;
+    real* out = p.imfs + (int64_t)MAXI * off;
     TimeAxis T;
     T.arange = p.t_mode == kTArange;
     T.T = p.t_mode == kTShared ? p.T : (p.t_mode == kTPerTrace ? p.T + off : nullptr);
 
     if (fixed_bytes<NT, kGImf>(N) + kRedBytes + 64 > (size_t)p.arena_bytes ||
-        (kWide && p.q_off + (size_t)N * sizeof(double) > p.slab_stride) ||
-        (kGImf && p.imf_off + (size_t)N * sizeof(double) > p.slab_stride)) {
+        (kWide && p.q_off + (size_t)N * sizeof(real) > p.slab_stride) ||
+        (kGImf && p.imf_off + (size_t)N * sizeof(real) > p.slab_stride)) {
       // cannot hold this trace: report, leave outputs flagged
       if (tid == 0) {
         atomicOr(p.status, kStatusTooLong);
@@ -1656,7 +1687,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     }
     SmemLayout L = carve<NT, kGImf>(smem, N, p.arena_bytes, gimf);
     Ctl& C = *L.ctl;
-    double* imf = L.imf;
+    real* imf = L.imf;
     for (int k = tid; k < MAXI; k += NT) { C.dbg_n[k] = -1; C.dbg_e[k] = -1; C.dbg_z[k] = -1; }
 #if EMDB_LOAD_CLOCKS
     const long long clk_trace0 = clock64();
@@ -1755,8 +1786,8 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         const bool f2 = abs(extNo2 - nzm2) < 2;
         bool f1 = false;
         if (!pass_bad) {
-          double sum_new_sq = C.sums[0], diff_sq = C.sums[1], old_sq = C.sums[2];
-          double std_sum = C.sums[3], omax = C.sums[4], omin = C.sums[5];
+          real sum_new_sq = C.sums[0], diff_sq = C.sums[1], old_sq = C.sums[2];
+          real std_sum = C.sums[3], omax = C.sums[4], omin = C.sums[5];
           if (sum_new_sq < kSumNewSqMin) f1 = false;
           else if (diff_sq / (omax - omin) < kSvarThr) f1 = true;
           else if (std_sum < kStdThr) f1 = true;
@@ -1771,28 +1802,28 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
       // ---- emit IMF row, running residue into the next row, end condition ----
       EMDB_PH(&C, 9);
       {
-        const double* rsrc = imf_count == 0 ? S : out + (int64_t)imf_count * N;
-        double* row = out + (int64_t)imf_count * N;
-        double* rnext = out + (int64_t)(imf_count + 1) * N;
-        double gmax = -1e30, gmin = 1e30, gabs = 0.0;
+        const real* rsrc = imf_count == 0 ? S : out + (int64_t)imf_count * N;
+        real* row = out + (int64_t)imf_count * N;
+        real* rnext = out + (int64_t)(imf_count + 1) * N;
+        real gmax = -1e30, gmin = 1e30, gabs = 0.0;
         // the reference's 128 lanes (a wider CTA's other threads wait: once per IMF)
         for (int i = tid; i < (!kWide || tid < kThreads ? N : 0); i += kThreads) {
-          double r = rsrc[i];
-          double v = imf[i];
+          real r = rsrc[i];
+          real v = imf[i];
           row[i] = v;
-          double rn = r - v;
+          real rn = r - v;
           rnext[i] = rn;
           gmax = fmax(gmax, rn);
           gmin = fmin(gmin, rn);
           gabs += fabs(rn);
         }
-        double* red = L.red;
+        real* red = L.red;
         if (!kWide || tid < kThreads) { red[tid] = gmax; red[128 + tid] = gmin; red[256 + tid] = gabs; }
         __syncthreads();
         if (warp == 0) {
-          double a0 = lane_tree(red, lane, 1);
-          double a1 = lane_tree(red + 128, lane, 2);
-          double a2 = lane_tree(red + 256, lane, 0);
+          real a0 = lane_tree(red, lane, 1);
+          real a1 = lane_tree(red + 128, lane, 2);
+          real a2 = lane_tree(red + 256, lane, 0);
           if (lane == 0) { C.sums[6] = a0 - a1; C.sums[7] = a2; }
         }
         __syncthreads();
@@ -1800,7 +1831,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         if (C.sums[6] < kRangeThr || C.sums[7] < kTotalPowerThr) finished = true;
       }
       if (!finished && imf_count < MAXI - 1) {
-        const double* rsrc = out + (int64_t)imf_count * N;
+        const real* rsrc = out + (int64_t)imf_count * N;
         for (int i = tid; i < N; i += NT) imf[i] = rsrc[i];
         __syncthreads();
         e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
@@ -1813,18 +1844,18 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     const int last_row = imf_count;   // row holding the running residue (or none if 0 IMFs)
     const bool trend = extNo_last <= 2 && imf_count > 0;
     if (trend) imf_count -= 1;
-    const double* rres = last_row == 0 ? S : out + (int64_t)last_row * N;
-    double amax = 0.0;
+    const real* rres = last_row == 0 ? S : out + (int64_t)last_row * N;
+    real amax = 0.0;
     for (int i = tid; i < (!kWide || tid < kThreads ? N : 0); i += kThreads) {
-      double r = rres[i];
+      real r = rres[i];
       if (trend) r = r + imf[i];
       amax = fmax(amax, fabs(r));
     }
-    double* red = L.red;
+    real* red = L.red;
     if (!kWide || tid < kThreads) red[tid] = amax;
     __syncthreads();
     if (warp == 0) {
-      double a = lane_tree(red, lane, 1);
+      real a = lane_tree(red, lane, 1);
       if (lane == 0) C.sums[0] = a;
     }
     __syncthreads();
@@ -1832,7 +1863,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     const int nim = rzero ? imf_count : imf_count + 1;
     for (int i = tid; i < N; i += NT) {
       if (trend) {
-        double r = rres[i] + imf[i];
+        real r = rres[i] + imf[i];
         if (!rzero) out[(int64_t)imf_count * N + i] = r;
         out[(int64_t)last_row * N + i] = 0.0;
       } else {
@@ -1878,8 +1909,8 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
 template <bool kSmem>
 __device__ __forceinline__ void envelope_pass(const SmemLayout& L, char* slab, const ExtInfo& e,
                                               int N, int NB, const TimeAxis& T, int tid, int warp,
-                                              int lane, double* emax_out, double* emin_out,
-                                              double* kp[2], double* kv[2], int mbuf, int nk[2],
+                                              int lane, real* emax_out, real* emin_out,
+                                              real* kp[2], real* kv[2], int mbuf, int nk[2],
                                               int* status) {
   Ctl& C = *L.ctl;
   const int kc0 = e.n_max + 2 * NB + 2, kc1 = e.n_min + 2 * NB + 2;
@@ -1900,13 +1931,13 @@ __device__ __forceinline__ void envelope_pass(const SmemLayout& L, char* slab, c
   const int kcnt[2] = {kn0, kn1};
   bool oor = false;
   for (int i = tid; i < N; i += kThreads) {
-    double t = T(i);
+    real t = T(i);
     int lo0 = sv[0].n >= 4 ? search_seg(sv[0], t) : 0;
     int lo1 = sv[1].n >= 4 ? search_seg(sv[1], t) : 0;
     bool r0 = !(t < sv[0].x[0] || t > sv[0].x[sv[0].n - 1]);
     bool r1 = !(t < sv[1].x[0] || t > sv[1].x[sv[1].n - 1]);
-    double a = eval_seg(sv[0], t, lo0);
-    double c = eval_seg(sv[1], t, lo1);
+    real a = eval_seg(sv[0], t, lo0);
+    real c = eval_seg(sv[1], t, lo1);
     emax_out[i] = r0 ? a : 0.0;
     emin_out[i] = r1 ? c : 0.0;
     oor |= !(r0 && r1);
@@ -1932,11 +1963,11 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
     if (b >= p.batch) break;
     const int64_t off = p.offsets ? p.offsets[b] : (int64_t)b * p.dense_n;
     const int N = p.offsets ? (int)(p.offsets[b + 1] - off) : p.dense_n;
-    const double* S = p.values + off;
-    double* emax_out = p.max_env + off;
-    double* emin_out = p.min_env + off;
-    double* kp[2] = {p.max_kpos + (int64_t)b * p.mbuf, p.min_kpos + (int64_t)b * p.mbuf};
-    double* kv[2] = {p.max_kval + (int64_t)b * p.mbuf, p.min_kval + (int64_t)b * p.mbuf};
+    const real* S = p.values + off;
+    real* emax_out = p.max_env + off;
+    real* emin_out = p.min_env + off;
+    real* kp[2] = {p.max_kpos + (int64_t)b * p.mbuf, p.min_kpos + (int64_t)b * p.mbuf};
+    real* kv[2] = {p.max_kval + (int64_t)b * p.mbuf, p.min_kval + (int64_t)b * p.mbuf};
     TimeAxis T;
     T.arange = p.t_mode == kTArange;
     T.T = p.t_mode == kTShared ? p.T : (p.t_mode == kTPerTrace ? p.T + off : nullptr);
@@ -1980,6 +2011,7 @@ __global__ void __launch_bounds__(kThreads, 4) emd_envelope_kernel(EnvParams p) 
   }
 }
 
+#if !EMDB_F32
 // ---------------------------------------------------------------------------
 // Self-test of div_rn against the hardware division.  mode 0: every integer
 // pair 0 <= a <= b <= n (the operands of A and B on the default time axis,
@@ -2069,6 +2101,7 @@ cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
   div_check_kernel<<<148 * 8, 256, 0, stream>>>(mode, n, seed, mismatches);
   return cudaGetLastError();
 }
+#endif
 
 size_t sift_fixed_smem(int N, int variant, bool imf_global) {
   const int nt = variant_threads(variant);
@@ -2088,7 +2121,7 @@ size_t sift_slab_bytes(int max_extrema, int nbsym) {
   const long long kc = (long long)max_extrema + 2LL * nbsym + 2;
   const size_t cap = (size_t)(2 * kc);
   const size_t red_extra = (EMDB_FAST_DIV != 1 && 4 * cap >= (size_t)kRedDoubles) ? 0 : kRedBytes;
-  return align16(10 * cap * sizeof(double) + red_extra);
+  return align16(10 * cap * sizeof(real) + red_extra);
 }
 
 namespace {
@@ -2127,11 +2160,13 @@ cudaError_t launch_v(const SiftParams& p, int grid, cudaStream_t stream) {
 }
 }  // namespace
 
+#if !EMDB_F32
 bool sift_variant_ok(int v) { return v == 1 || v == 2 || v == 4 || v == 5 || v == 6; }
 
 int variant_threads(int v) {
   return v == 1 ? kWideThreads : v == 2 ? kHalfWideThreads : kThreads;
 }
+#endif
 
 cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm, bool imf_global) {
   switch (variant) {

@@ -113,16 +113,45 @@ struct DeviceGuard {
 // traces) 38.4 ms at 4 vs 42.2 ms at 3; N = 4096 within a few percent either
 // way, depending on the batch (81 vs 99 ms at 3 vs 4 CTAs/SM for 2,048
 // traces, 223 vs 218 ms for 8,192).
+// The sift kernels per value type: the FP64 build (the reference's REAL_T)
+// and the FP32 build of the same source.
+template <typename R> struct SiftKernels;
+template <> struct SiftKernels<double> {
+  using Params = emdb::SiftParams;
+  static size_t fixed_smem(int N, int variant, bool g = false) {
+    return emdb::sift_fixed_smem(N, variant, g);
+  }
+  static cudaError_t occupancy(int arena, int variant, int* per_sm, bool g = false) {
+    return emdb::sift_occupancy(arena, variant, per_sm, g);
+  }
+  static cudaError_t launch(const Params& sp, int grid, cudaStream_t st) {
+    return emdb::launch_sift(sp, grid, st);
+  }
+};
+template <> struct SiftKernels<float> {
+  using Params = emdb::f32::SiftParams;
+  static size_t fixed_smem(int N, int variant, bool g = false) {
+    return emdb::f32::sift_fixed_smem(N, variant, g);
+  }
+  static cudaError_t occupancy(int arena, int variant, int* per_sm, bool g = false) {
+    return emdb::f32::sift_occupancy(arena, variant, per_sm, g);
+  }
+  static cudaError_t launch(const Params& sp, int grid, cudaStream_t st) {
+    return emdb::f32::launch_sift(sp, grid, st);
+  }
+};
+
+template <typename R = double>
 int auto_arena_for(int smem_optin, int variant, int nbsym, int max_n) {
   const int per_sm = 233472;
-  const size_t fixed = emdb::sift_fixed_smem(std::max(max_n, 1), variant);
+  const size_t fixed = SiftKernels<R>::fixed_smem(std::max(max_n, 1), variant);
   auto share = [&](int want) {
     int arena = std::min(per_sm / want - 1024, smem_optin);
     // shared memory is allocated in 128-byte units: a 16-byte-rounded share
     // can round up past the SM's capacity and lose a CTA (e.g. 5 per SM)
     return arena & ~127;
   };
-  const size_t knot_room = (size_t)(11 * 2 * (96 + 2 * nbsym + 2)) * sizeof(double);
+  const size_t knot_room = (size_t)(11 * 2 * (96 + 2 * nbsym + 2)) * sizeof(R);
   for (int want = variant; want >= 1; --want)
     if ((size_t)share(want) >= fixed + knot_room) {
       if (want >= 3) return share(want);
@@ -147,13 +176,15 @@ int effective_variant(const emdb_plan* p, int max_n) {
   return max_n > 4096 ? 1 : max_n > 2048 ? 2 : 4;
 }
 
+template <typename R = double>
 int auto_arena(const emdb_plan* p, int max_n) {
-  return auto_arena_for(p->smem_optin, effective_variant(p, max_n), p->cfg.nbsym, max_n);
+  return auto_arena_for<R>(p->smem_optin, effective_variant(p, max_n), p->cfg.nbsym, max_n);
 }
 
+template <typename R = double>
 int arena_for(const emdb_plan* p, int max_n) {
   if (p->arena_override > 0) return p->arena_override;
-  return auto_arena(p, max_n);
+  return auto_arena<R>(p, max_n);
 }
 
 int ensure_slab(emdb_plan* p, size_t bytes) {
@@ -246,14 +277,16 @@ class ZeroRows {
 // masks are 16-bit, so at most 2^17 samples (< 2^16 extrema of a kind).
 constexpr int kMaxTraceLen = 1 << 17;
 
-int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
+template <typename R>
+int prepare_sift(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, int* grid) {
+  using K = SiftKernels<R>;
   if (max_n > kMaxTraceLen)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
                 " exceeds the longest supported trace (131072 samples)");
   int variant = effective_variant(p, max_n);
-  int arena = arena_for(p, max_n);
+  int arena = arena_for<R>(p, max_n);
   bool gimf = false;
-  if ((arena <= 0 || emdb::sift_fixed_smem(max_n, variant) + 64 > (size_t)arena) &&
+  if ((arena <= 0 || K::fixed_smem(max_n, variant) + 64 > (size_t)arena) &&
       p->arena_override == 0) {
     // Too long for the plan's instance (at its automatic arena; an explicit
     // arena that cannot hold the trace is the caller's error, below): the
@@ -263,13 +296,13 @@ int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
     // shared memory while it fits, else in the CTA's global slab.
     variant = 1;
     arena = p->smem_optin & ~127;
-    gimf = emdb::sift_fixed_smem(max_n, 1) + 64 > (size_t)arena;
+    gimf = K::fixed_smem(max_n, 1) + 64 > (size_t)arena;
   }
-  if (arena <= 0 || emdb::sift_fixed_smem(max_n, variant, gimf) + 64 > (size_t)arena)
+  if (arena <= 0 || K::fixed_smem(max_n, variant, gimf) + 64 > (size_t)arena)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
                 " does not fit this device's shared memory");
   int per_sm = 0;
-  cudaError_t e = emdb::sift_occupancy(arena, variant, &per_sm, gimf);
+  cudaError_t e = K::occupancy(arena, variant, &per_sm, gimf);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
   *grid = std::min(sp.batch, per_sm * p->num_sms);
@@ -283,7 +316,7 @@ int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
     // the wide instance parks the proto-IMF and keeps the stop-test
     // quotients in two trace-length arrays after the knot slab (and, for a
     // trace longer than shared memory holds, the proto-IMF itself after them)
-    const size_t trace = al256((size_t)std::max(max_n, 1) * sizeof(double));
+    const size_t trace = al256((size_t)std::max(max_n, 1) * sizeof(R));
     sp.park_off = al256(p->slab_stride);
     sp.q_off = sp.park_off + trace;
     sp.slab_stride = sp.q_off + trace;
@@ -300,9 +333,10 @@ int prepare_sift(emdb_plan* p, emdb::SiftParams& sp, int max_n, int* grid) {
   return EMDB_OK;
 }
 
-int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st) {
+template <typename R = double>
+int launch_common(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, cudaStream_t st) {
   int grid = 0;
-  int rc = prepare_sift(p, sp, max_n, &grid);
+  int rc = prepare_sift<R>(p, sp, max_n, &grid);
   if (rc) return rc;
   rc = ensure_slab(p, sp.slab_stride * (size_t)grid);
   if (rc) return rc;
@@ -310,7 +344,7 @@ int launch_common(emdb_plan* p, emdb::SiftParams& sp, int max_n, cudaStream_t st
   sp.slab = p->d_slab;
   cudaError_t e = cudaMemsetAsync(p->d_ctl, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_fail(e, "queue reset");
-  e = emdb::launch_sift(sp, grid, st);
+  e = SiftKernels<R>::launch(sp, grid, st);
   if (e != cudaSuccess) return cuda_fail(e, "sift launch");
   return EMDB_OK;
 }
@@ -416,19 +450,34 @@ int emdb_plan_set_max_ctas(emdb_plan* p, int max_ctas) {
   return EMDB_OK;
 }
 
-int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm, int* grid_max) {
+}  // extern "C"
+
+template <typename R>
+static int plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm,
+                      int* grid_max) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   DeviceGuard g(p->device);
-  int arena = arena_for(p, max_n);
+  int arena = arena_for<R>(p, max_n);
   int per_sm = 0;
   if (arena > 0) {
-    cudaError_t e = emdb::sift_occupancy(arena, effective_variant(p, max_n), &per_sm);
+    cudaError_t e = SiftKernels<R>::occupancy(arena, effective_variant(p, max_n), &per_sm);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   }
   if (arena_bytes) *arena_bytes = arena;
   if (ctas_per_sm) *ctas_per_sm = per_sm;
   if (grid_max) *grid_max = per_sm * p->num_sms;
   return EMDB_OK;
+}
+
+extern "C" {
+
+int emdb_plan_query(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm, int* grid_max) {
+  return plan_query<double>(p, max_n, arena_bytes, ctas_per_sm, grid_max);
+}
+
+int emdb_plan_query_f32(emdb_plan* p, int max_n, int* arena_bytes, int* ctas_per_sm,
+                        int* grid_max) {
+  return plan_query<float>(p, max_n, arena_bytes, ctas_per_sm, grid_max);
 }
 
 int emdb_host_bytes(emdb_plan* p, unsigned long long* h2d, unsigned long long* d2h) {
@@ -459,10 +508,12 @@ int emdb_pass_placement(const emdb_config* cfg, int N, int arena_bytes, int n_ma
   return EMDB_OK;
 }
 
-int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, int N,
-             double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
-             void* stream) {
-  NvtxRange nvtx_range("emdb_run");
+}  // extern "C"
+
+namespace {
+template <typename R>
+int run_dense(emdb_plan* p, const R* signals, const R* T, int batch, int N, R* imfs, int* n_imfs,
+              int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm, void* stream) {
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
   if (batch == 0) return EMDB_OK;
@@ -470,7 +521,7 @@ int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, in
     return fail(EMDB_ERR_INVALID, "NULL buffer");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
-  emdb::SiftParams sp{};
+  typename SiftKernels<R>::Params sp{};
   sp.values = signals;
   sp.offsets = nullptr;
   sp.dense_n = N;
@@ -484,7 +535,26 @@ int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, in
   sp.dbg_n = dbg_n;
   sp.dbg_ext = dbg_extno;
   sp.dbg_nzm = dbg_nzm;
-  return launch_common(p, sp, N, (cudaStream_t)stream);
+  return launch_common<R>(p, sp, N, (cudaStream_t)stream);
+}
+}  // namespace
+
+extern "C" {
+
+int emdb_run(emdb_plan* p, const double* signals, const double* T, int batch, int N,
+             double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
+             void* stream) {
+  NvtxRange nvtx_range("emdb_run");
+  return run_dense<double>(p, signals, T, batch, N, imfs, n_imfs, overflow, dbg_n, dbg_extno,
+                           dbg_nzm, stream);
+}
+
+int emdb_run_f32(emdb_plan* p, const float* signals, const float* T, int batch, int N,
+                 float* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                 int* dbg_nzm, void* stream) {
+  NvtxRange nvtx_range("emdb_run_f32");
+  return run_dense<float>(p, signals, T, batch, N, imfs, n_imfs, overflow, dbg_n, dbg_extno,
+                          dbg_nzm, stream);
 }
 
 int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batch, int N,
@@ -570,7 +640,7 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
     c += gchunks[k];
     emdb::SiftParams sp = base;
     sp.batch = gcount[k];
-    int rc = prepare_sift(p, sp, N, &grid[k]);
+    int rc = prepare_sift<double>(p, sp, N, &grid[k]);
     if (rc) return rc;
     if (k == 0) base = sp;                     // arena and config fields are shared
   }
@@ -701,11 +771,14 @@ int emdb_run_host(emdb_plan* p, const double* signals, const double* T, int batc
   return EMDB_OK;
 }
 
-static int run_ragged_impl(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
-                           int max_n, const double* T, int t_per_trace, const int* order,
-                           double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+}  // extern "C"
+
+template <typename R>
+static int run_ragged_impl(emdb_plan* p, const R* values, const int64_t* offsets, int batch,
+                           int max_n, const R* T, int t_per_trace, const int* order,
+                           R* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                            int* dbg_nzm, emdb_notify* nt, int n_traces, void* stream) {
-  NvtxRange nvtx_range("emdb_run_ragged");
+  NvtxRange nvtx_range(sizeof(R) == 4 ? "emdb_run_ragged_f32" : "emdb_run_ragged");
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || max_n < 0) return fail(EMDB_ERR_INVALID, "batch and max_n must be >= 0");
   if (batch == 0) return EMDB_OK;
@@ -715,7 +788,7 @@ static int run_ragged_impl(emdb_plan* p, const double* values, const int64_t* of
     return fail(EMDB_ERR_INVALID, "notify object too small or on another device");
   std::lock_guard<std::mutex> lk(p->mu);
   DeviceGuard g(p->device);
-  emdb::SiftParams sp{};
+  typename SiftKernels<R>::Params sp{};
   sp.values = values;
   sp.offsets = offsets;
   sp.dense_n = 0;
@@ -736,15 +809,25 @@ static int run_ragged_impl(emdb_plan* p, const double* values, const int64_t* of
     sp.chunk_traces = 1;
     sp.chunk_span = n_traces;
   }
-  return launch_common(p, sp, max_n, (cudaStream_t)stream);
+  return launch_common<R>(p, sp, max_n, (cudaStream_t)stream);
 }
+
+extern "C" {
 
 int emdb_run_ragged(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
                     int max_n, const double* T, int t_per_trace, const int* order, double* imfs,
                     int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
                     void* stream) {
-  return run_ragged_impl(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs, n_imfs,
-                         overflow, dbg_n, dbg_extno, dbg_nzm, nullptr, 0, stream);
+  return run_ragged_impl<double>(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs,
+                                 n_imfs, overflow, dbg_n, dbg_extno, dbg_nzm, nullptr, 0, stream);
+}
+
+int emdb_run_ragged_f32(emdb_plan* p, const float* values, const int64_t* offsets, int batch,
+                        int max_n, const float* T, int t_per_trace, const int* order, float* imfs,
+                        int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno, int* dbg_nzm,
+                        void* stream) {
+  return run_ragged_impl<float>(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs,
+                                n_imfs, overflow, dbg_n, dbg_extno, dbg_nzm, nullptr, 0, stream);
 }
 
 int emdb_run_ragged_notify(emdb_plan* p, const double* values, const int64_t* offsets, int batch,
@@ -752,8 +835,9 @@ int emdb_run_ragged_notify(emdb_plan* p, const double* values, const int64_t* of
                            double* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
                            int* dbg_nzm, emdb_notify* notify, int n_traces, void* stream) {
   if (!notify) return fail(EMDB_ERR_INVALID, "notify is NULL");
-  return run_ragged_impl(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs, n_imfs,
-                         overflow, dbg_n, dbg_extno, dbg_nzm, notify, n_traces, stream);
+  return run_ragged_impl<double>(p, values, offsets, batch, max_n, T, t_per_trace, order, imfs,
+                                 n_imfs, overflow, dbg_n, dbg_extno, dbg_nzm, notify, n_traces,
+                                 stream);
 }
 
 int emdb_notify_create(int capacity, int device, emdb_notify** out, unsigned** host_flags) {
@@ -805,11 +889,36 @@ int emdb_notify_destroy(emdb_notify* nt) {
   return EMDB_OK;
 }
 
-int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batch, int N,
-                  double* max_env, double* min_env, int* n_extrema, int* degenerate,
-                  double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
-                  int* n_mirrored, void* stream) {
-  NvtxRange nvtx_range("emdb_envelope");
+}  // extern "C"
+
+namespace {
+template <typename R> struct EnvKernels;
+template <> struct EnvKernels<double> {
+  using Params = emdb::EnvParams;
+  static size_t fixed_smem(int N) { return emdb::sift_fixed_smem(N); }
+  static cudaError_t occupancy(int arena, int* per_sm) {
+    return emdb::envelope_occupancy(arena, per_sm);
+  }
+  static cudaError_t launch(const Params& ep, int grid, cudaStream_t st) {
+    return emdb::launch_envelope(ep, grid, st);
+  }
+};
+template <> struct EnvKernels<float> {
+  using Params = emdb::f32::EnvParams;
+  static size_t fixed_smem(int N) { return emdb::f32::sift_fixed_smem(N); }
+  static cudaError_t occupancy(int arena, int* per_sm) {
+    return emdb::f32::envelope_occupancy(arena, per_sm);
+  }
+  static cudaError_t launch(const Params& ep, int grid, cudaStream_t st) {
+    return emdb::f32::launch_envelope(ep, grid, st);
+  }
+};
+
+template <typename R>
+int run_envelope(emdb_plan* p, const R* signals, const R* T, int batch, int N, R* max_env,
+                 R* min_env, int* n_extrema, int* degenerate, R* max_kpos, R* max_kval,
+                 R* min_kpos, R* min_kval, int* n_mirrored, void* stream) {
+  using K = EnvKernels<R>;
   if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
   if (batch < 0 || N < 0) return fail(EMDB_ERR_INVALID, "batch and N must be >= 0");
   if (batch == 0) return EMDB_OK;
@@ -822,18 +931,19 @@ int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batc
   // the envelope kernel has 128-thread CTAs: the arena rule of that instance
   // unless the plan names another
   int arena = p->arena_override > 0 ? p->arena_override
-                                    : auto_arena_for(p->smem_optin, p->variant ? p->variant : 4,
-                                                     p->cfg.nbsym, N);
-  if (arena <= 0 || emdb::sift_fixed_smem(N) + 64 > (size_t)arena)
+                                    : auto_arena_for<R>(p->smem_optin,
+                                                        p->variant ? p->variant : 4,
+                                                        p->cfg.nbsym, N);
+  if (arena <= 0 || K::fixed_smem(N) + 64 > (size_t)arena)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length does not fit this device's shared memory");
   int per_sm = 0;
-  cudaError_t e = emdb::envelope_occupancy(arena, &per_sm);
+  cudaError_t e = K::occupancy(arena, &per_sm);
   if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
   if (per_sm < 1) return fail(EMDB_ERR_UNSUPPORTED, "kernel cannot be resident with this arena");
   int grid = std::min(batch, per_sm * p->num_sms);
   int rc = ensure_slab(p, p->slab_stride * (size_t)grid);
   if (rc) return rc;
-  emdb::EnvParams ep{};
+  typename K::Params ep{};
   ep.values = signals;
   ep.offsets = nullptr;
   ep.dense_n = N;
@@ -859,9 +969,30 @@ int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batc
   ep.nbsym = p->cfg.nbsym;
   e = cudaMemsetAsync(p->d_ctl + 2, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_fail(e, "queue reset");
-  e = emdb::launch_envelope(ep, grid, st);
+  e = K::launch(ep, grid, st);
   if (e != cudaSuccess) return cuda_fail(e, "envelope launch");
   return EMDB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int emdb_envelope(emdb_plan* p, const double* signals, const double* T, int batch, int N,
+                  double* max_env, double* min_env, int* n_extrema, int* degenerate,
+                  double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
+                  int* n_mirrored, void* stream) {
+  NvtxRange nvtx_range("emdb_envelope");
+  return run_envelope<double>(p, signals, T, batch, N, max_env, min_env, n_extrema, degenerate,
+                              max_kpos, max_kval, min_kpos, min_kval, n_mirrored, stream);
+}
+
+int emdb_envelope_f32(emdb_plan* p, const float* signals, const float* T, int batch, int N,
+                      float* max_env, float* min_env, int* n_extrema, int* degenerate,
+                      float* max_kpos, float* max_kval, float* min_kpos, float* min_kval,
+                      int* n_mirrored, void* stream) {
+  NvtxRange nvtx_range("emdb_envelope_f32");
+  return run_envelope<float>(p, signals, T, batch, N, max_env, min_env, n_extrema, degenerate,
+                             max_kpos, max_kval, min_kpos, min_kval, n_mirrored, stream);
 }
 
 int emdb_plan_counters(emdb_plan* p, unsigned long long* passes, unsigned long long* spilled,

@@ -25,17 +25,20 @@ enum : int {
 // Time axis modes.
 enum : int { kTArange = 0, kTShared = 1, kTPerTrace = 2 };
 
-struct SiftParams {
+// R: the type the sift computes in -- double (the reference's REAL_T), or
+// float for the FP32 build of the same kernel source (namespace emdb::f32).
+template <typename R>
+struct SiftParamsT {
   // input: CSR traces (dense [B,N] is offsets b*N)
-  const double* values;
+  const R* values;
   const int64_t* offsets;     // [batch+1], or NULL for a dense [batch, dense_n] batch
   int dense_n;
-  const double* T;            // per t_mode
+  const R* T;                 // per t_mode
   int t_mode;
   int batch;
   const int* order;           // queue order (NULL = FIFO)
   // outputs: trace b's rows start at imfs + max_imfs*offsets[b], row r at +r*N_b
-  double* imfs;
+  R* imfs;
   int* n_imfs;
   int* overflow;
   int* dbg_n;
@@ -69,21 +72,22 @@ struct SiftParams {
                               // 2: 256-thread CTAs, two per SM
 };
 
-struct EnvParams {
-  const double* values;
+template <typename R>
+struct EnvParamsT {
+  const R* values;
   const int64_t* offsets;     // NULL = dense [batch, dense_n]
   int dense_n;
-  const double* T;
+  const R* T;
   int t_mode;
   int batch;
-  double* max_env;            // CSR like values
-  double* min_env;
+  R* max_env;                 // CSR like values
+  R* min_env;
   int* n_extrema;             // [batch,2]
   int* degenerate;            // [batch]
-  double* max_kpos;           // [batch, mbuf]
-  double* max_kval;
-  double* min_kpos;
-  double* min_kval;
+  R* max_kpos;                // [batch, mbuf]
+  R* max_kval;
+  R* min_kpos;
+  R* min_kval;
   int* n_mirrored;            // [batch,2]
   int mbuf;
   int* queue;
@@ -94,6 +98,9 @@ struct EnvParams {
   int max_extrema;
   int nbsym;
 };
+
+using SiftParams = SiftParamsT<double>;
+using EnvParams = EnvParamsT<double>;
 
 // Shared-memory bytes a CTA of the given variant needs beyond the knot arena
 // for a trace of length N (imf_global: the wide instance with the proto-IMF in
@@ -117,5 +124,22 @@ cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm,
 cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm);
 cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
                              unsigned long long* mismatches, cudaStream_t stream);
+
+// The FP32 build of the sift and envelope kernels (emd_sift.cu compiled with
+// EMDB_F32=1): the same algorithm in float, with the reference kernel's mixed
+// float / double expressions (its source compiled with REAL_T = float).  Sizes
+// count 4-byte values.
+namespace f32 {
+using SiftParams = SiftParamsT<float>;
+using EnvParams = EnvParamsT<float>;
+size_t sift_fixed_smem(int N, int variant = 4, bool imf_global = false);
+size_t sift_slab_bytes(int max_extrema, int nbsym);
+int sift_pass_placement(int N, int arena_total, size_t slab_stride, int kc0, int kc1);
+cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream);
+cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream);
+cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm,
+                           bool imf_global = false);
+cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm);
+}  // namespace f32
 
 }  // namespace emdb

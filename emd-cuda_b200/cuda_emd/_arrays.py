@@ -53,6 +53,18 @@ def as_device_f64(x, device: int):
     return t, k
 
 
+def as_device_real(x, device: int, f32: bool):
+    """Device tensor of the launcher's value type (float64, or float32 for
+    the FP32 kernels); any other dtype raises."""
+    if not f32:
+        return as_device_f64(x, device)
+    torch = _torch()
+    t, k = _to_torch(x, device)
+    if t.dtype != torch.float32:
+        raise ValueError(f"expected float32, got {t.dtype}")
+    return t, k
+
+
 def as_device_i64(x, device: int):
     torch = _torch()
     t, _ = _to_torch(x, device)

@@ -36,7 +36,8 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_host_bytes", "emdb_host_register", "emdb_host_unregister",
            "emdb_notify_create", "emdb_notify_reset", "emdb_notify_destroy",
            "emdb_run_ragged_notify", "emdb_pass_placement", "emdb_noalloc_status",
-           "emdb_pack_rows")
+           "emdb_pack_rows", "emdb_run_f32", "emdb_run_ragged_f32", "emdb_envelope_f32",
+           "emdb_plan_query_f32")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -72,6 +73,9 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_phase_clocks.argtypes = [VP, P, I, I]
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
+        L.emdb_run_f32.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
+        L.emdb_plan_query_f32.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I),
+                                          ctypes.POINTER(I)]
         L.emdb_run_host.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
         L.emdb_min_arena.argtypes = [I, ctypes.POINTER(I)]
         L.emdb_notify_create.argtypes = [I, I, ctypes.POINTER(VP),
@@ -84,7 +88,9 @@ def load() -> ctypes.CDLL:
         L.emdb_host_bytes.argtypes = [VP, ctypes.POINTER(ctypes.c_ulonglong),
                                       ctypes.POINTER(ctypes.c_ulonglong)]
         L.emdb_run_ragged.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]
+        L.emdb_run_ragged_f32.argtypes = [VP, P, P, I, I, P, I, P, P, P, P, P, P, P, VP]
         L.emdb_envelope.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
+        L.emdb_envelope_f32.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, P, P, P, VP]
         L.emdb_status.argtypes = [VP, ctypes.POINTER(I), VP]
         L.emdb_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
         L.emdb_run_noalloc.argtypes = [ctypes.POINTER(EmdbConfig), P, P, I, I, P, P, P, P, P, P, VP]
@@ -195,10 +201,13 @@ class Plan:
     def set_max_ctas(self, max_ctas: int) -> None:
         check(self.L.emdb_plan_set_max_ctas(self.handle, int(max_ctas)), "emdb_plan_set_max_ctas")
 
-    def query(self, max_n: int) -> tuple[int, int, int]:
+    def query(self, max_n: int, f32: bool = False) -> tuple[int, int, int]:
+        """(arena bytes, CTAs per SM, grid) the plan's launches use for traces
+        up to max_n (f32: the FP32 kernels)."""
         a, c, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        check(self.L.emdb_plan_query(self.handle, int(max_n), ctypes.byref(a), ctypes.byref(c),
-                                     ctypes.byref(g)), "emdb_plan_query")
+        fn = self.L.emdb_plan_query_f32 if f32 else self.L.emdb_plan_query
+        check(fn(self.handle, int(max_n), ctypes.byref(a), ctypes.byref(c), ctypes.byref(g)),
+              "emdb_plan_query")
         return a.value, c.value, g.value
 
     def host_bytes(self) -> tuple[int, int]:

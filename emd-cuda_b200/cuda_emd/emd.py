@@ -26,34 +26,70 @@ except ImportError:  # flat layout: emd.py and kernels.py side by side
     from kernels import EMDKernelConfig  # type: ignore
 
 
-def _normalise_T(T, N: int, device: int):
+# FP32 path: the largest normalised time a float axis may hold, so that every
+# sample time and mirrored knot position (up to about twice the last time)
+# keeps a spacing of at least one ulp.  The reference drops a knot whose
+# position equals its neighbour's (kernels.py:521-556); with such an axis that
+# never happens, as in double.
+F32_MAX_TIME = float(1 << 22)
+
+
+def _as_f64_axis(T, device: int, f32: bool):
+    # the reference normalises T in float64 whatever it was given
+    # (cp.asarray(T, dtype=cp.float64), emd.py:85); the FP64 launcher keeps
+    # its dtype rule (float64 only), the FP32 one also takes float32 T
+    from ._arrays import as_device_f64, _to_torch
+    if not f32:
+        return as_device_f64(T, device)[0]
+    import torch
+    t, _ = _to_torch(T, device)
+    if t.dtype not in (torch.float32, torch.float64):
+        raise ValueError(f"T must be float32 or float64, got {t.dtype}")
+    return t.to(torch.float64)
+
+
+def _to_real(Tn, f32: bool):
+    """The normalised axis in the kernels' type; for float it must stay
+    strictly increasing and below F32_MAX_TIME."""
+    if not f32:
+        return Tn
+    import torch
+    Tf = Tn.to(torch.float32)
+    if Tf.numel() > 1 and not bool((Tf[1:] > Tf[:-1]).all()):
+        raise ValueError("T must normalise to an axis that stays strictly increasing in float32")
+    if Tf.numel() and float(Tf.abs().max().item()) >= F32_MAX_TIME:
+        raise ValueError(f"normalised T must stay below {F32_MAX_TIME:.0f} for REAL_T=float")
+    return Tf
+
+
+def _normalise_T(T, N: int, device: int, f32: bool = False):
     """emd.py:83-88: arange(N) if T is None, else (T - T[0]) / min(diff(T)).
     None stays None (the kernel then uses arange without a buffer).  The
     normalised axis must be finite and strictly increasing; the reference
-    would read stale envelope values otherwise, so this build refuses it."""
+    would read stale envelope values otherwise, so this build refuses it.
+    f32: normalised in float64 as the reference does, then rounded to float."""
     if T is None:
         return None
     import torch
-    from ._arrays import as_device_f64
-    Td, _ = as_device_f64(T, device)
+    Td = _as_f64_axis(T, device, f32)
     if Td.dim() != 1 or Td.shape[0] != N:
         raise ValueError(f"T must be 1-D of length {N}")
     if N < 2:
-        return Td - Td[0] if N == 1 else Td
+        return _to_real(Td - Td[0] if N == 1 else Td, f32)
     d = Td[1:] - Td[:-1]
     Tn = (Td - Td[0]) / torch.min(d)
     dn = Tn[1:] - Tn[:-1]
     if not bool(torch.isfinite(Tn).all()) or not bool((dn > 0).all()):
         raise ValueError("T must normalise to a finite, strictly increasing axis")
-    return Tn
+    return _to_real(Tn, f32)
 
 
-def _normalise_T_csr(T, offsets, device: int):
+def _normalise_T_csr(T, offsets, device: int, f32: bool = False):
     """Per-trace _normalise_T of CSR-aligned time axes, on the device:
     (T_b - T_b[0]) / min(diff(T_b)) for every trace b."""
     import torch
-    from ._arrays import as_device_f64, as_device_i64
-    Td, _ = as_device_f64(T, device)
+    from ._arrays import as_device_i64
+    Td = _as_f64_axis(T, device, f32)
     offs = as_device_i64(offsets, device)
     if Td.dim() != 1 or Td.shape[0] != int(offs[-1].item()):
         raise ValueError("T must be 1-D and aligned with values (length offsets[-1])")
@@ -71,6 +107,13 @@ def _normalise_T_csr(T, offsets, device: int):
     dn = Tn[1:] - Tn[:-1]
     if not bool(torch.isfinite(Tn).all()) or not bool((dn[inner] > 0).all()):
         raise ValueError("each trace's T must normalise to a finite, strictly increasing axis")
+    if f32:
+        Tf = Tn.to(torch.float32)
+        if not bool((Tf[1:] > Tf[:-1])[inner].all()):
+            raise ValueError("each trace's T must stay strictly increasing in float32")
+        if Tf.numel() and float(Tf.abs().max().item()) >= F32_MAX_TIME:
+            raise ValueError(f"normalised T must stay below {F32_MAX_TIME:.0f} for REAL_T=float")
+        return Tf
     return Tn
 
 
@@ -88,7 +131,8 @@ class GPUBatchEMD:
         """One tiny real call (an all-zero trace, emd.py:58-64) so that plan
         creation and first-launch costs land here, not in a timed call."""
         import torch
-        self(torch.zeros((1, N), dtype=torch.float64, device="cuda"))
+        dt = torch.float32 if self._config.f32 else torch.float64
+        self(torch.zeros((1, N), dtype=dt, device="cuda"))
 
     def _get_launcher(self):
         if self._launcher is None:
@@ -108,35 +152,56 @@ class GPUBatchEMD:
                 stacklevel=3,
             )
 
-    def __call__(self, signals, T=None, out=None):
+    def __call__(self, signals, T=None, out=None, order=None):
         """Decompose signals [batch, N] (or [N]).  Device input (torch CUDA,
         CuPy) gives device results.  Host input (NumPy, CPU torch) runs the
         host pipeline: one launch whose finished traces are copied back while
         the rest sift, results in host memory; ``out`` = optional
-        (imfs, n_imfs, overflow) host buffers to fill."""
+        (imfs, n_imfs, overflow) host buffers to fill.  ``order`` (device
+        input only): an int32 permutation of the batch giving the work
+        queue's order (e.g. scheduler.learned_order's longest-predicted-first);
+        it changes when each trace runs, never a result."""
         if signals.ndim == 1:
             signals = signals[None, :]
         dt = np.dtype(str(signals.dtype).replace("torch.", ""))
-        if dt != np.dtype(np.float64):
+        if dt != self._config.dtype:
             raise ValueError(
-                f"GPUBatchEMD (this build) is float64 only, got {signals.dtype}. "
-                f"Cast explicitly first, e.g. signals.astype(float64) -- this "
+                f"GPUBatchEMD (this build) is {self._config.dtype} only, got {signals.dtype}. "
+                f"Cast explicitly first, e.g. signals.astype({self._config.dtype}) -- this "
                 f"class won't silently do that for you."
             )
         launcher = self._get_launcher()
         batch, N = signals.shape
-        Tn = _normalise_T(T, N, launcher.device)
+        Tn = _normalise_T(T, N, launcher.device, self._config.f32)
         from ._arrays import kind_of
         if kind_of(signals) in ("numpy", "torch_cpu"):
+            if order is not None:
+                raise ValueError("order= is for device input")
             imfs, n_imfs, overflow, dn, de, dz = launcher.run_host(signals, Tn, out=out)
         elif out is not None:
             raise ValueError("out= is for host input; device input returns device arrays")
+        elif order is not None:
+            imfs, n_imfs, overflow, dn, de, dz = self._run_ordered(launcher, signals, Tn, order)
         else:
             imfs, n_imfs, overflow, dn, de, dz = launcher.run(signals, Tn)
         self.last_debug = (dn, de, dz)
         launcher.check_status()
         self._overflow_warning(overflow, batch)
         return imfs, n_imfs, overflow
+
+    @staticmethod
+    def _run_ordered(launcher, signals, Tn, order):
+        """A dense batch through the CSR launch (offsets b*N), whose queue
+        takes an order: trace b's rows land at b*max_imfs*N, the dense layout."""
+        import torch
+        from ._arrays import _to_torch
+        sig, _ = _to_torch(signals, launcher.device)
+        B, N = sig.shape
+        offs = torch.arange(0, (B + 1) * N, N, dtype=torch.int64, device=sig.device)
+        res = launcher.run_ragged(sig.reshape(-1), offs, order=order, T=Tn,
+                                  t_per_trace=False, max_n=N)
+        mi = launcher.config.max_imfs
+        return (res[0].reshape(B, mi, N),) + tuple(res[1:])
 
     def ragged(self, values, offsets, T=None, order=None, max_n: int | None = None):
         """Decompose a CSR batch (values f64 [total], offsets int64 [batch+1]) in
@@ -147,7 +212,7 @@ class GPUBatchEMD:
         permutation) only sets the queue order.  Returns (imfs_csr, n_imfs,
         overflow)."""
         launcher = self._get_launcher()
-        Tn = None if T is None else _normalise_T_csr(T, offsets, launcher.device)
+        Tn = None if T is None else _normalise_T_csr(T, offsets, launcher.device, self._config.f32)
         imfs, n_imfs, overflow, dn, de, dz = launcher.run_ragged(values, offsets, order=order,
                                                                  T=Tn, t_per_trace=True,
                                                                  max_n=max_n)

@@ -14,8 +14,10 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _native
-from ._arrays import (as_device_f64, as_device_i64, as_device_i32, to_caller, device_of, stream_of,
-                      kind_of)
+from ._arrays import (as_device_f64, as_device_real, as_device_i64, as_device_i32, to_caller,
+                      device_of, stream_of, kind_of)
+
+REAL_TYPES = {"double": np.float64, "float": np.float32}
 
 
 @dataclass
@@ -25,15 +27,27 @@ class EMDKernelConfig:
     max_iteration: int = 1000
     max_imfs: int = 16
     threads_per_block: int = 128
+    # The type the kernels compute in: the reference substitutes REAL_T into
+    # its kernel source from this name (kernels.py:78, 1277-1285) and fixes
+    # it to "double"; "float" selects the FP32 build of the B200 kernels.
+    real_t: str = "double"
+
+    def __post_init__(self):
+        if self.real_t not in REAL_TYPES:
+            raise ValueError(f"real_t must be one of {sorted(REAL_TYPES)}, got {self.real_t!r}")
 
     @property
     def dtype(self):
-        return np.dtype(np.float64)
+        return np.dtype(REAL_TYPES[self.real_t])
 
     @property
     def real_t_name(self) -> str:
         """The C type the kernels compute in (kernels.py:1182-1185)."""
-        return "double"
+        return self.real_t
+
+    @property
+    def f32(self) -> bool:
+        return self.real_t == "float"
 
     @property
     def itemsize(self) -> int:
@@ -47,7 +61,7 @@ class EMDKernelConfig:
 
     @classmethod
     def for_device(cls, device=None, target_blocks_per_sm: int = 4,
-                   min_max_extrema: int = 1024) -> "EMDKernelConfig":
+                   min_max_extrema: int = 1024, real_t: str = "double") -> "EMDKernelConfig":
         """Same sizing arithmetic as the reference (kernels.py:1205-1271), so
         the default ``max_extrema`` -- which decides the overflow flag and the
         extrema truncation -- matches it on the same device (1024 on B200)."""
@@ -56,7 +70,7 @@ class EMDKernelConfig:
                            (device.index if device is not None and hasattr(device, "index") and device.index is not None
                             else torch.cuda.current_device()))
         optin = _smem_optin(dev.index)
-        cfg = cls()
+        cfg = cls(real_t=real_t)
         static_bytes = cfg.static_shared_mem_bytes()
         per_elem = 6 * cfg.itemsize + 2 * 4
         budget_occ = max(0, optin // target_blocks_per_sm - static_bytes)
@@ -74,7 +88,7 @@ class EMDKernelConfig:
 
     def arena_bytes(self, max_n: int, device: int | None = None) -> int:
         """Dynamic shared memory per CTA the B200 kernel uses for traces up to max_n."""
-        return self.build(device)._plan.query(max_n)[0]
+        return self.build(device)._plan.query(max_n, f32=self.f32)[0]
 
     def to_c(self) -> _native.EmdbConfig:
         return _native.EmdbConfig(int(self.max_extrema), int(self.nbsym), int(self.max_iteration),
@@ -129,20 +143,22 @@ class EMDBatchLauncher:
         (kernels.py:1343-1372)."""
         import torch
         self._check_dtype(signals, T)
-        sig, kind = as_device_f64(signals, self.device)
+        f32 = self.config.f32
+        sig, kind = as_device_real(signals, self.device, f32)
         if sig.dim() != 2:
             raise ValueError("signals must be [batch, N]")
-        Td = None if T is None else as_device_f64(T, self.device)[0]
+        Td = None if T is None else as_device_real(T, self.device, f32)[0]
         B, N = sig.shape
         mi = self.config.max_imfs
-        imfs = torch.empty((B, mi, N), dtype=torch.float64, device=sig.device)
+        imfs = torch.empty((B, mi, N), dtype=sig.dtype, device=sig.device)
         n_imfs = torch.empty(B, dtype=torch.int32, device=sig.device)
         ovf = torch.empty(B, dtype=torch.int32, device=sig.device)
         dn = torch.empty((B, mi), dtype=torch.int32, device=sig.device)
         de = torch.empty((B, mi), dtype=torch.int32, device=sig.device)
         dz = torch.empty((B, mi), dtype=torch.int32, device=sig.device)
         st = stream_of(sig.device)
-        _native.check(self._plan.L.emdb_run(
+        fn = self._plan.L.emdb_run_f32 if f32 else self._plan.L.emdb_run
+        _native.check(fn(
             self._plan.handle, sig.data_ptr(), Td.data_ptr() if Td is not None else None, B, N,
             imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(), dn.data_ptr(), de.data_ptr(),
             dz.data_ptr(), st), "emdb_run")
@@ -158,6 +174,9 @@ class EMDBatchLauncher:
         as run(), in the caller's framework."""
         import torch
         self._check_dtype(signals, T)
+        if self.config.f32:
+            raise ValueError("the host-memory pipeline computes in double; for REAL_T=float "
+                             "copy the batch to the device and call run()")
         kind = kind_of(signals)
         if kind not in ("numpy", "torch_cpu"):
             raise ValueError("run_host takes host arrays (NumPy or CPU torch)")
@@ -201,23 +220,25 @@ class EMDBatchLauncher:
         (imfs_csr [max_imfs * total], n_imfs, overflow, debug_n, debug_extno, debug_nzm);
         trace b's rows are imfs_csr[max_imfs*off[b] : max_imfs*off[b+1]].reshape(max_imfs, N_b)."""
         import torch
-        vals, kind = as_device_f64(values, self.device)
+        f32 = self.config.f32
+        vals, kind = as_device_real(values, self.device, f32)
         offs = as_device_i64(offsets, self.device)
         B = offs.shape[0] - 1
         if max_n is None:
             max_n = int((offs[1:] - offs[:-1]).max().item()) if B > 0 else 0
-        Td = None if T is None else as_device_f64(T, self.device)[0]
+        Td = None if T is None else as_device_real(T, self.device, f32)[0]
         od = None if order is None else as_device_i32(order, self.device)
         mi = self.config.max_imfs
         total = vals.shape[0]
-        imfs = torch.empty(mi * total, dtype=torch.float64, device=vals.device)
+        imfs = torch.empty(mi * total, dtype=vals.dtype, device=vals.device)
         n_imfs = torch.empty(B, dtype=torch.int32, device=vals.device)
         ovf = torch.empty(B, dtype=torch.int32, device=vals.device)
         dn = torch.empty((B, mi), dtype=torch.int32, device=vals.device)
         de = torch.empty((B, mi), dtype=torch.int32, device=vals.device)
         dz = torch.empty((B, mi), dtype=torch.int32, device=vals.device)
         st = stream_of(vals.device)
-        _native.check(self._plan.L.emdb_run_ragged(
+        fn = self._plan.L.emdb_run_ragged_f32 if f32 else self._plan.L.emdb_run_ragged
+        _native.check(fn(
             self._plan.handle, vals.data_ptr(), offs.data_ptr(), B, int(max_n),
             Td.data_ptr() if Td is not None else None, 1 if t_per_trace else 0,
             od.data_ptr() if od is not None else None, imfs.data_ptr(), n_imfs.data_ptr(),
@@ -230,16 +251,18 @@ class EMDBatchLauncher:
         9-tuple (kernels.py:1374-1407)."""
         import torch
         self._check_dtype(signals, T)
-        sig, kind = as_device_f64(signals, self.device)
-        Td = None if T is None else as_device_f64(T, self.device)[0]
+        f32 = self.config.f32
+        sig, kind = as_device_real(signals, self.device, f32)
+        Td = None if T is None else as_device_real(T, self.device, f32)[0]
         B, N = sig.shape
         mbuf = self.config.max_extrema + 2 * self.config.nbsym
         dev = sig.device
-        f = lambda *s: torch.empty(s, dtype=torch.float64, device=dev)
+        f = lambda *s: torch.empty(s, dtype=sig.dtype, device=dev)
         i = lambda *s: torch.empty(s, dtype=torch.int32, device=dev)
         outs = (f(B, N), f(B, N), i(B, 2), i(B), f(B, mbuf), f(B, mbuf), f(B, mbuf), f(B, mbuf), i(B, 2))
         st = stream_of(dev)
-        _native.check(self._plan.L.emdb_envelope(
+        fn = self._plan.L.emdb_envelope_f32 if f32 else self._plan.L.emdb_envelope
+        _native.check(fn(
             self._plan.handle, sig.data_ptr(), Td.data_ptr() if Td is not None else None, B, N,
             *[o.data_ptr() for o in outs], st), "emdb_envelope")
         self._keepalive = (sig, Td)

@@ -224,3 +224,14 @@ def lpt_order(cost):
     """Longest-predicted-first permutation (int32) for the work queue."""
     import torch
     return torch.argsort(cost, descending=True, stable=True).to(torch.int32)
+
+
+def learned_order(model: CostModel, signals):
+    """Queue order for a dense device batch [batch, N]: features, the BF16
+    cost model and longest-predicted-first, all on the device.  Pass it as
+    GPUBatchEMD(...)(signals, order=...)."""
+    import torch
+    X = signals if signals.dtype == torch.float64 else signals.to(torch.float64)
+    B, N = X.shape
+    lengths = torch.full((B,), N, dtype=torch.int64, device=X.device)
+    return lpt_order(predicted_cost(model, features(X), lengths))

@@ -188,6 +188,34 @@ int emdb_envelope(emdb_plan* plan, const double* signals, const double* T, int b
                   double* max_kpos, double* max_kval, double* min_kpos, double* min_kval,
                   int* n_mirrored, void* stream);
 
+/* FP32 path: the same entry points computing in float.  The reference's
+ * kernel source is written over REAL_T (kernels.py:78), substituted from
+ * EMDKernelConfig.real_t_name when it is built (kernels.py:1277-1285); its
+ * Python layer fixes that to double.  These run the reference algorithm with
+ * REAL_T = float: every array and REAL_T variable is float, and the
+ * source's double literals keep their C++ meaning (an expression such as
+ * the envelope's "... * (h * h) / 6.0" is evaluated in double and rounded
+ * once to float; "sum < 1e-10" compares in double), bit for bit like that
+ * source built with REAL_T = float and -fmad=false.  Discrete outcomes
+ * (extrema counts, sift counts, IMF counts) can differ from the FP64 path.
+ * Arguments as for the FP64 entries, with float buffers; T must stay
+ * strictly increasing in float after normalisation. */
+int emdb_run_f32(emdb_plan* plan, const float* signals, const float* T, int batch, int N,
+                 float* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                 int* dbg_nzm, void* stream);
+int emdb_run_ragged_f32(emdb_plan* plan, const float* values, const int64_t* offsets, int batch,
+                        int max_n, const float* T, int t_per_trace, const int* order,
+                        float* imfs, int* n_imfs, int* overflow, int* dbg_n, int* dbg_extno,
+                        int* dbg_nzm, void* stream);
+int emdb_envelope_f32(emdb_plan* plan, const float* signals, const float* T, int batch, int N,
+                      float* max_env, float* min_env, int* n_extrema, int* degenerate,
+                      float* max_kpos, float* max_kval, float* min_kpos, float* min_kval,
+                      int* n_mirrored, void* stream);
+/* emdb_plan_query for the FP32 kernels (4-byte values: more knots on-chip,
+ * longer traces per CTA). */
+int emdb_plan_query_f32(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
+                        int* grid_max);
+
 /* Sift passes the plan's launches have run so far, and how many of them kept
  * their knots in the global spill slab instead of shared memory (tuning
  * diagnostics).  Synchronises the device; reset != 0 clears the counters. */
