@@ -114,22 +114,23 @@ def make_workload(name: str, rank: int = 0):
 # ---------------------------------------------------------------------------
 
 def _oracle_chunk(args):
-    X, = args
+    X, real_t = args
     sys.path.insert(0, ROOT)
     from oracle import emd_oracle as O
-    T = np.arange(X.shape[1], dtype=np.float64)
+    cfg = O.OracleConfig(real_t=real_t)
+    T = np.arange(X.shape[1], dtype=cfg.rtype)
     t0 = time.perf_counter()
     for x in X:
-        O.emd_signal(x, T)
+        O.emd_signal(x, T, cfg)
     return X.shape[0], time.perf_counter() - t0
 
 
-def cpu_oracle_rate(X: np.ndarray, pool, cores: int, sample: int):
+def cpu_oracle_rate(X: np.ndarray, pool, cores: int, sample: int, real_t: str = "double"):
     """signals/s of the oracle over `sample` traces split across `cores` processes."""
     sub = X[:sample]
     parts = [p for p in np.array_split(sub, cores) if p.shape[0]]
     t0 = time.perf_counter()
-    res = pool.map(_oracle_chunk, [(p,) for p in parts])
+    res = pool.map(_oracle_chunk, [(p, real_t) for p in parts])
     wall = time.perf_counter() - t0
     n = sum(r[0] for r in res)
     return n / wall, n, wall
@@ -201,12 +202,15 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dgemm_tflops(dev) -> float:
-    """FP64 peak measured here: cuBLAS DGEMM 8192^3, best of 5."""
+def dgemm_tflops(dev, dtype=None) -> float:
+    """FP64 peak measured here: cuBLAS DGEMM 8192^3, best of 5 (dtype float32:
+    SGEMM with TF32 off, the FP32 pipe's peak)."""
     import torch
+    dtype = dtype or torch.float64
+    torch.backends.cuda.matmul.allow_tf32 = False
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device=dev)
-    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
     torch.matmul(a, b)
     torch.cuda.synchronize(dev)
     best = 0.0
@@ -245,6 +249,12 @@ def main():
     ap.add_argument("--clocks-csv", default=None,
                     help="keep the raw clock samples here ({rank} = rank); default: a temp file")
     ap.add_argument("--variant", type=int, default=0, help="kernel register variant: min CTAs/SM")
+    ap.add_argument("--real", default="double", choices=["double", "float"],
+                    help="dense workloads: the type the kernels compute in (REAL_T)")
+    ap.add_argument("--order", default="fifo", choices=["fifo", "learned"],
+                    help="dense workloads: queue order of the timed steps (learned: the cost "
+                         "model, trained here on a disjoint seeded batch, orders each step's "
+                         "queue longest-predicted-first; the FIFO rate is reported beside it)")
     ap.add_argument("--train-traces", type=int, default=200000, help="ragged64k: MLP training set")
     ap.add_argument("--eval-traces", type=int, default=0, help="ragged64k: batch size (0 = 65536)")
     ap.add_argument("--epochs", type=int, default=20)
@@ -302,10 +312,16 @@ def main():
 
     from cuda_emd import GPUBatchEMD, EMDKernelConfig
 
+    import dataclasses
+    f32 = a.real == "float"
     X = make_workload(a.workload, rank)
+    if f32:
+        X = X.astype(np.float32)
     B, N = X.shape
+    isz = X.dtype.itemsize
     sig = torch.from_numpy(X).to(dev)
-    cfg = EMDKernelConfig.for_device(local)
+    # same config for both types (max_extrema as the FP64 sizing gives it)
+    cfg = dataclasses.replace(EMDKernelConfig.for_device(local), real_t=a.real)
     emd = GPUBatchEMD(cfg)
     emd.warmup()
     launcher = emd._get_launcher()
@@ -313,7 +329,7 @@ def main():
         launcher._plan.set_variant(a.variant)
     if a.arena:
         launcher._plan.set_arena(a.arena)
-    arena_used, ctas_per_sm, grid_max = launcher._plan.query(N)
+    arena_used, ctas_per_sm, grid_max = launcher._plan.query(N, f32=f32)
 
     # ---- device-resident throughput ----
     for _ in range(a.warmup):
@@ -327,7 +343,7 @@ def main():
     launcher.run(sig, None)
     passes_step, spilled_step = launcher._plan.counters(reset=True)
     flops_per_step = algorithmic_flops(N, n_imfs, dbg_n, dbg_ext)
-    hbm_bytes_per_step = 8.0 * B * N + 8.0 * B * cfg.max_imfs * N
+    hbm_bytes_per_step = float(isz) * B * N + float(isz) * B * cfg.max_imfs * N
 
     R.barrier(world)
     torch.cuda.synchronize(dev)
@@ -354,15 +370,83 @@ def main():
     ms_per_step = elapsed / a.steps * 1e3
     launch_s = statistics.mean(per_launch)
 
+    # ---- learned queue order (dense): features + BF16 MLP + LPT + launch per step ----
+    ordered = None
+    if a.order == "learned":
+        from cuda_emd import scheduler as S
+        t_tr = time.perf_counter()
+        Xtr = make_workload(a.workload, rank + 1000)         # same generator, disjoint seed
+        xtr = torch.from_numpy(Xtr).to(dev)
+        emd_tr = GPUBatchEMD(dataclasses.replace(cfg, real_t="double")) if f32 else emd
+        ltr = emd_tr._get_launcher()
+        otr = ltr.run(xtr, None)
+        cm = S.CostModel(dev, seed=0)
+        cm.fit(S.features(xtr), S.labels_from_debug(otr[3], otr[1]), epochs=30, batch=256)
+        cm.warmup()
+        del otr, xtr
+        torch.cuda.synchronize(dev)
+        train_s = time.perf_counter() - t_tr
+
+        def learned_step():
+            order = S.learned_order(cm, sig)
+            return GPUBatchEMD._run_ordered(launcher, sig, None, order)
+
+        true_cost = torch.from_numpy(np.where(dbg_n > 0, dbg_n, 0).sum(1).astype(np.float32)).to(dev)
+        true_order = S.lpt_order(true_cost)
+
+        def timed_order(fn):
+            for _ in range(max(1, min(a.warmup, 2))):
+                fn()
+            torch.cuda.synchronize(dev)
+            R.barrier(world)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(a.steps):
+                fn()
+            e1.record(st)
+            torch.cuda.synchronize(dev)
+            return R.max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
+
+        clocks2 = ClockSampler(local, None)
+        el_learned = timed_order(learned_step)
+        clk2 = clocks2.stop() if clocks2 else None
+        el_true = timed_order(lambda: GPUBatchEMD._run_ordered(launcher, sig, None, true_order))
+        chk = learned_step()
+        assert all(torch.equal(x, y) for x, y in
+                   zip(chk, launcher.run(sig, None))), "order changed a result"
+        del chk
+        ordered = {"plain_value": round(value, 2), "plain_ms_per_step": round(ms_per_step, 3),
+                   "learned_ms_per_step": round(el_learned / a.steps * 1e3, 3),
+                   "speedup_learned": round(elapsed / el_learned, 4),
+                   "true_cost_ms_per_step": round(el_true / a.steps * 1e3, 3),
+                   "speedup_true_cost": round(elapsed / el_true, 4),
+                   "train": f"{Xtr.shape[0]} traces of the same generator (disjoint seed), "
+                            f"30 epochs, {train_s:.1f} s",
+                   "note": "learned step = features + BF16 inference + LPT order + the launch, "
+                           "all inside the timed region; true-cost = the queue ordered by the "
+                           "logged sift passes (known only afterwards): the ordering ceiling",
+                   "clocks": clk2}
+        value = R.whole_job_rate(B, a.steps, world, el_learned)
+        ms_per_step = el_learned / a.steps * 1e3
+
     # ---- end to end through the public API with pinned host buffers ----
     e2e = None
     if not a.no_e2e:
         host_in = torch.from_numpy(X).pin_memory()
-        host_imfs = torch.empty((B, cfg.max_imfs, N), dtype=torch.float64).pin_memory()
+        host_imfs = torch.empty((B, cfg.max_imfs, N), dtype=sig.dtype).pin_memory()
         host_n = torch.empty(B, dtype=torch.int32).pin_memory()
         host_o = torch.empty(B, dtype=torch.int32).pin_memory()
 
         def e2e_step():
+            if f32:
+                # the FP32 path takes device arrays: the batch goes up, the
+                # public call sifts it, every result row comes back
+                d = host_in.to(dev, non_blocking=True)
+                im, nn, oo = emd(d)
+                host_imfs.copy_(im, non_blocking=True)
+                host_n.copy_(nn, non_blocking=True)
+                host_o.copy_(oo, non_blocking=True)
+                return
             # host input -> host results through GPUBatchEMD: the library copies
             # the batch up, sifts it in one launch and copies each finished
             # chunk of traces back while the rest still sift
@@ -378,14 +462,19 @@ def main():
         e1.record(st)
         torch.cuda.synchronize(dev)
         te = R.max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
-        h2d, d2h = emd._get_launcher()._plan.host_bytes()     # what the last step moved
+        if f32:
+            h2d, d2h = isz * B * N, isz * B * cfg.max_imfs * N + 8 * B
+        else:
+            h2d, d2h = emd._get_launcher()._plan.host_bytes()     # what the last step moved
         e2e = {"value": R.whole_job_rate(B, a.steps, world, te), "unit": "signals/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "d2h_dense_bytes_per_step": int(8 * B * cfg.max_imfs * N + 8 * B
+               "d2h_dense_bytes_per_step": int(isz * B * cfg.max_imfs * N + 8 * B
                                                + 3 * 4 * B * cfg.max_imfs),
-               "note": "of each finished chunk only the rows that may hold data are "
-                       "copied; the zero rows after them are written on the host, "
-                       "inside the timed region"}
+               "note": ("device copy of the batch, GPUBatchEMD on it, every output row "
+                        "copied back" if f32 else
+                        "of each finished chunk only the rows that may hold data are "
+                        "copied; the zero rows after them are written on the host, "
+                        "inside the timed region")}
         del host_imfs
 
     # ---- roofline ----
@@ -395,17 +484,19 @@ def main():
         pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
         if os.path.isfile(pk):
             peaks = json.load(open(pk))
-        fp64 = dgemm_tflops(dev)
+        fp64 = dgemm_tflops(dev, torch.float32 if f32 else torch.float64)
         achieved = flops_per_step / launch_s / 1e12
         hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
         hbm_ach = hbm_bytes_per_step / launch_s / 1e9
-        per_trace = NCU_DRAM_BYTES_PER_TRACE.get((N, cfg.max_imfs))
+        per_trace = None if f32 else NCU_DRAM_BYTES_PER_TRACE.get((N, cfg.max_imfs))
         traffic = round(per_trace * B) if per_trace else None
-        roofline = {"bound": "fp64", "achieved": round(achieved, 3), "peak": round(fp64, 3),
+        roofline = {"bound": "fp32" if f32 else "fp64", "achieved": round(achieved, 3),
+                    "peak": round(fp64, 3),
                     "unit": "TFLOP/s", "frac": round(achieved / fp64, 4), "traffic": traffic,
                     "traffic_source": ("ncu dram__bytes_read+write per trace of a 1024-trace "
                                        "launch x traces per launch") if traffic else None,
-                    "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                    "peak_source": ("cuBLAS SGEMM (TF32 off) 8192^3 measured in this run" if f32
+                                    else "cuBLAS DGEMM 8192^3 measured in this run"),
                     "kernel": "emd_sift_kernel",
                     "algorithmic_flop_per_launch": flops_per_step,
                     "launch_ms": round(launch_s * 1e3, 3),
@@ -418,7 +509,7 @@ def main():
     cpu = None
     if pool is not None:
         sample = a.cpu_sample or max(cores * 128, 64)
-        rate, n, wall = cpu_oracle_rate(X, pool, cores, min(sample, B))
+        rate, n, wall = cpu_oracle_rate(X, pool, cores, min(sample, B), a.real)
         cpu = {"value": round(rate, 2), "unit": "signals/s", "cores": cores, "kind": "port",
                "sample": f"first {n} traces of the workload, NumPy oracle, {cores} processes, "
                          f"{wall:.1f} s wall"}
@@ -426,20 +517,26 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "signals/s", "n_gpus": world,
+            "metric": METRIC.replace("FP64", "FP32") if f32 else METRIC, "value": round(value, 2),
+            "unit": "signals/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_per_step, 3),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if f32 else "f64",
             "data": "synthetic (seeded generator, see cuda_emd/workloads.py)",
             "config": {"workload": a.workload, "desc": WORKLOADS[a.workload]["desc"],
                        "batch_per_gpu": B, "N": N, "max_imfs": cfg.max_imfs,
                        "max_extrema": cfg.max_extrema, "max_iteration": cfg.max_iteration,
-                       "queue": "FIFO persistent", "l2": "inputs+outputs larger than L2",
+                       "queue": ("learned longest-predicted-first" if ordered
+                                 else "FIFO persistent"),
+                       "l2": "inputs+outputs larger than L2",
+                       "real_t": a.real,
                        "arena_bytes": arena_used, "ctas_per_sm": ctas_per_sm,
                        "sift_passes_per_step": passes_step,
                        "spilled_pass_frac": round(spilled_step / max(passes_step, 1), 4),
                        "overflow_traces": ovf, "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": a.steps,
+            "order": ordered,
+            "gpu_launches": a.steps * (3 if ordered else 1),
         }
         print(json.dumps(line), flush=True)
     R.finish(world)

@@ -23,7 +23,11 @@ recipe does the same job with nvcc:
      arithmetic the NumPy oracle restates bit for bit;
    * ``libemd_ref_small[_nofma].so`` -- MAX_EXTREMA=128, MAX_ITERATION=6, so
      that short fixtures reach both overflow paths (extrema cap and
-     iteration cap).
+     iteration cap);
+   * ``libemd_ref[_small]_f32[_nofma].so`` -- the same source with REAL_T =
+     float (the substitution key the reference's build takes from
+     ``EMDKernelConfig.real_t_name``, kernels.py:1284; its Python layer fixes
+     it to double): the pin of the FP32 path.
 
 The extracted source never lands in the repository.  Run:
 ``python oracle/build_ref.py --ref <reference checkout>`` (or set
@@ -47,14 +51,20 @@ DEFAULT_REF = os.environ.get("EMDB_REFERENCE_DIR", "")
 DEFAULTS = dict(MAX_EXTREMA=1024, NBSYM=2, MAX_ITERATION=1000, MAX_IMFS=16, THREADS=128,
                 REAL_T="double")
 SMALL = dict(MAX_EXTREMA=128, MAX_ITERATION=6)
+F32 = dict(REAL_T="float")
 VARIANTS = (
     ("libemd_ref.so", {}, []),
     ("libemd_ref_nofma.so", {}, ["-fmad=false"]),
     ("libemd_ref_small.so", SMALL, []),
     ("libemd_ref_small_nofma.so", SMALL, ["-fmad=false"]),
+    ("libemd_ref_f32.so", F32, []),
+    ("libemd_ref_f32_nofma.so", F32, ["-fmad=false"]),
+    ("libemd_ref_small_f32.so", dict(SMALL, **F32), []),
+    ("libemd_ref_small_f32_nofma.so", dict(SMALL, **F32), ["-fmad=false"]),
 )
 
-# Host-side launcher written for this recipe (not part of the reference).
+# Host-side launcher written for this recipe (not part of the reference); its
+# buffers are REAL_T, the type the reference source #defines (kernels.py:78).
 LAUNCHER = r"""
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -70,9 +80,11 @@ extern "C" int ref_config(int* out5) {
     return 0;
 }
 
-extern "C" int ref_emd_launch(const double* signals, const double* T, int batch, int N,
-                              double* imfs, int* n_imfs, int* overflow,
-                              double* pools6, int* dbg_n, int* dbg_ext, int* dbg_nzm,
+extern "C" int ref_real_bytes(void) { return (int)sizeof(REAL_T); }
+
+extern "C" int ref_emd_launch(const REAL_T* signals, const REAL_T* T, int batch, int N,
+                              REAL_T* imfs, int* n_imfs, int* overflow,
+                              REAL_T* pools6, int* dbg_n, int* dbg_ext, int* dbg_nzm,
                               cudaStream_t stream) {
     size_t smem = ref_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(emd_batch_kernel,
@@ -87,10 +99,10 @@ extern "C" int ref_emd_launch(const double* signals, const double* T, int batch,
     return (int)cudaGetLastError();
 }
 
-extern "C" int ref_envelope_launch(const double* signals, const double* T, int batch, int N,
-                                   double* max_env, double* min_env, int* n_extrema,
-                                   int* degenerate, double* max_kpos, double* max_kval,
-                                   double* min_kpos, double* min_kval, int* n_mirrored,
+extern "C" int ref_envelope_launch(const REAL_T* signals, const REAL_T* T, int batch, int N,
+                                   REAL_T* max_env, REAL_T* min_env, int* n_extrema,
+                                   int* degenerate, REAL_T* max_kpos, REAL_T* max_kval,
+                                   REAL_T* min_kpos, REAL_T* min_kval, int* n_mirrored,
                                    cudaStream_t stream) {
     size_t smem = ref_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(envelope_batch_kernel,

@@ -37,6 +37,23 @@ multiply-add, so this equals a CUDA build with FMA contraction off.
 Parity pinning: ``tests/golden/`` holds outputs of the reference's own
 ``emd_batch_kernel`` (compiled from kernels.py by ``oracle/build_ref.py`` and
 run on a B200); ``tests/test_oracle_golden.py`` checks this oracle against them.
+
+REAL_T = float
+---------------
+The reference's kernel source is written over ``REAL_T`` (kernels.py:78),
+substituted when it is built (kernels.py:1277-1285).  With
+``OracleConfig(real_t="float")`` every array and REAL_T variable here is
+float32 and the source's double literals keep their C++ meaning: a float
+expression that meets one is evaluated in double and rounded once when it is
+stored (the mirrored positions ``2.0 * T[a] - T[b]``, kernels.py:471-489,
+528-553; the spline rows' ``h0 + 2.0 * h1``, kernels.py:551, 558; the
+evaluation's ``... * (h * h) / 6.0``, kernels.py:733), and the two tests
+against double literals compare in double (``sum_new_sq < 1e-10``,
+kernels.py:814; ``<= 1e-8``, kernels.py:1069).  Where float arithmetic and that
+double detour give the same value (a product by 2.0 or 6.0 of a float, a
+float compared with 0.0) the float form is used.  NumPy's float32 operations
+round every step (NEP 50 keeps Python scalars weak), as a CUDA build without
+FMA contraction does.
 """
 from __future__ import annotations
 
@@ -60,13 +77,19 @@ LOCAL_EXT_BUF = 64
 
 @dataclass
 class OracleConfig:
-    """Mirror of the reference's ``EMDKernelConfig`` fields (kernels.py:1170-1176)."""
+    """Mirror of the reference's ``EMDKernelConfig`` fields (kernels.py:1170-1176),
+    plus the REAL_T its kernel source is built with."""
 
     max_extrema: int = 1024
     nbsym: int = 2
     max_iteration: int = 1000
     max_imfs: int = 16
     threads_per_block: int = 128
+    real_t: str = "double"
+
+    @property
+    def rtype(self):
+        return np.float32 if self.real_t == "float" else np.float64
 
 
 @dataclass
@@ -98,27 +121,34 @@ def lane_sum(x: np.ndarray, lanes: int = 128) -> float:
     (e.g. kernels.py:777-804, 1016-1033).  Terms must be >= 0 or NaN (all the
     reference's sums are), so the zero padding is exact."""
     n = x.shape[0]
+    dt = x.dtype if x.dtype == np.float32 else np.float64
     rows = -(-n // lanes) if n else 1
-    buf = np.zeros(rows * lanes, dtype=np.float64)
+    buf = np.zeros(rows * lanes, dtype=dt)
     buf[:n] = x
     grid = buf.reshape(rows, lanes)
-    acc = np.zeros(lanes, dtype=np.float64)
+    acc = np.zeros(lanes, dtype=dt)
     for r in range(rows):
         acc = acc + grid[r]
     s = lanes // 2
     while s > 0:
         acc[:s] = acc[:s] + acc[s:2 * s]
         s //= 2
-    return float(acc[0])
+    return acc[0] if dt == np.float32 else float(acc[0])
 
 
-def lane_max(x: np.ndarray, init: float = -1e30) -> float:
-    """max over samples with the reference's -1e30 seed; CUDA max(double) is fmax."""
-    return float(np.fmax.reduce(x, initial=init)) if x.size else init
+def _scalar(v, dt):
+    return v if dt == np.float32 else float(v)
 
 
-def lane_min(x: np.ndarray, init: float = 1e30) -> float:
-    return float(np.fmin.reduce(x, initial=init)) if x.size else init
+def lane_max(x: np.ndarray, init: float = -1e30):
+    """max over samples with the reference's -1e30 seed (a REAL_T); CUDA max is fmax."""
+    dt = x.dtype.type
+    return _scalar(np.fmax.reduce(x, initial=dt(init)) if x.size else dt(init), dt)
+
+
+def lane_min(x: np.ndarray, init: float = 1e30):
+    dt = x.dtype.type
+    return _scalar(np.fmin.reduce(x, initial=dt(init)) if x.size else dt(init), dt)
 
 
 # ---------------------------------------------------------------------------
@@ -128,7 +158,9 @@ def lane_min(x: np.ndarray, init: float = 1e30) -> float:
 def _extrema_serial(S: np.ndarray, max_extrema: int):
     """Literal restatement of find_extrema_serial (kernels.py:115-204)."""
     N = S.shape[0]
-    s = S.tolist()
+    # float32 samples stay float32 scalars (their differences and products
+    # round to float, as REAL_T = float does); float64 ones become Python floats
+    s = list(S) if S.dtype == np.float32 else S.tolist()
     n_zer = 0
     in_zero_run = False
     for i in range(N):
@@ -285,10 +317,13 @@ def mirror_knots(T: np.ndarray, S: np.ndarray, ind_max: np.ndarray, ind_min: np.
     lmin_fb, rmin_fb = len(lmin) == 0, len(rmin) == 0
     lmax_fb, rmax_fb = len(lmax) == 0, len(rmax) == 0
     # ---- "mirrored point does not reach the boundary" (kernels.py:469-503) ----
+    R = T.dtype.type
+    # REAL_T x = 2.0 * T[a] - T[b]: formed in double, stored as REAL_T
+    mpos = lambda a, b: R(2.0 * float(T[a]) - float(T[b]))
     lmin_first = iN[0] if lmin_fb else lmin[0]
     lmax_first = im[0] if lmax_fb else lmax[0]
-    tlmin0 = 2.0 * T[lsym] - T[lmin_first]
-    tlmax0 = 2.0 * T[lsym] - T[lmax_first]
+    tlmin0 = mpos(lsym, lmin_first)
+    tlmax0 = mpos(lsym, lmax_first)
     if tlmin0 > T[0] or tlmax0 > T[0]:
         if lsym == im[0]:
             lmax = [im[k] for k in range(min(n_max, NB) - 1, -1, -1)]
@@ -299,8 +334,8 @@ def mirror_knots(T: np.ndarray, S: np.ndarray, ind_max: np.ndarray, ind_min: np.
         lsym = 0
     rmin_last = iN[n_min - 1] if rmin_fb else rmin[-1]
     rmax_last = im[n_max - 1] if rmax_fb else rmax[-1]
-    trmin_last = 2.0 * T[rsym] - T[rmin_last]
-    trmax_last = 2.0 * T[rsym] - T[rmax_last]
+    trmin_last = mpos(rsym, rmin_last)
+    trmax_last = mpos(rsym, rmax_last)
     if trmin_last < T[N - 1] or trmax_last < T[N - 1]:
         if rsym == im[n_max - 1]:
             rmax = [im[k] for k in range(n_max - 1, max(n_max - NB, 0) - 1, -1)]
@@ -316,7 +351,9 @@ def mirror_knots(T: np.ndarray, S: np.ndarray, ind_max: np.ndarray, ind_min: np.
         li = np.asarray(li, dtype=np.int64)
         ri = np.asarray(ri, dtype=np.int64)
         ti = np.asarray(true_idx, dtype=np.int64)
-        pos = np.concatenate([2.0 * T[lsym] - T[li], T[ti], 2.0 * T[rsym] - T[ri]])
+        T64 = T.astype(np.float64)
+        pos = np.concatenate([(2.0 * T64[lsym] - T64[li]).astype(R), T[ti],
+                              (2.0 * T64[rsym] - T64[ri]).astype(R)])
         val = np.concatenate([S[li], S[ti], S[ri]])
         # keep a knot unless its position equals the previous one (kernels.py:521-556)
         keep = np.ones(pos.shape[0], dtype=bool)
@@ -340,10 +377,11 @@ def spline_moments(x: np.ndarray, y: np.ndarray) -> np.ndarray:
     (kernels.py:683-689) and end recovery (kernels.py:691-696)."""
     n = x.shape[0]
     m = n - 2
-    a = np.empty(m)
-    b = np.empty(m)
-    c = np.empty(m)
-    d = np.empty(m)
+    R = x.dtype.type
+    a = np.empty(m, dtype=R)
+    b = np.empty(m, dtype=R)
+    c = np.empty(m, dtype=R)
+    d = np.empty(m, dtype=R)
     with np.errstate(all="ignore"):
         # interior rows k in [1, m-2] -> original row i = k+1
         if m > 2:
@@ -358,14 +396,14 @@ def spline_moments(x: np.ndarray, y: np.ndarray) -> np.ndarray:
         h1 = x[2] - x[1]
         rhs1 = 6.0 * ((y[2] - y[1]) / h1 - (y[1] - y[0]) / h0)
         a[0] = 0.0
-        b[0] = h0 + 2.0 * h1
+        b[0] = R(float(h0) + 2.0 * float(h1))          # double literal: formed in double
         c[0] = h1 - h0
         d[0] = h1 * rhs1 / (h0 + h1)
         hnm3 = x[n - 2] - x[n - 3]
         hnm2 = x[n - 1] - x[n - 2]
         rhs_nm2 = 6.0 * ((y[n - 1] - y[n - 2]) / hnm2 - (y[n - 2] - y[n - 3]) / hnm3)
         a[m - 1] = hnm3 - hnm2
-        b[m - 1] = 2.0 * hnm3 + hnm2
+        b[m - 1] = R(2.0 * float(hnm3) + float(hnm2))
         c[m - 1] = 0.0
         d[m - 1] = hnm3 * rhs_nm2 / (hnm3 + hnm2)
         if m == 1:  # unreachable for n >= 4; kept for shape safety
@@ -393,7 +431,7 @@ def spline_moments(x: np.ndarray, y: np.ndarray) -> np.ndarray:
             nd = d - alpha * d_left - beta * d_right
             a, b, c, d = na, nb, nc, nd
             s *= 2
-        M = np.empty(n)
+        M = np.empty(n, dtype=R)
         M[1:n - 1] = d / b
         M[0] = ((h0 + h1) * M[1] - h0 * M[2]) / h1
         M[n - 1] = ((hnm3 + hnm2) * M[n - 2] - hnm2 * M[n - 3]) / hnm3
@@ -407,7 +445,7 @@ def spline_eval(T: np.ndarray, x: np.ndarray, y: np.ndarray, M: np.ndarray | Non
     n = x.shape[0]
     t = T
     in_range = ~((t < x[0]) | (t > x[n - 1]))
-    out = np.zeros(t.shape[0])
+    out = np.zeros(t.shape[0], dtype=x.dtype)
     with np.errstate(all="ignore"):
         if n == 2:
             slope = (y[1] - y[0]) / (x[1] - x[0])
@@ -437,7 +475,14 @@ def spline_eval(T: np.ndarray, x: np.ndarray, y: np.ndarray, M: np.ndarray | Non
             h = x1 - x0
             A = (x1 - t) / h
             B = (t - x0) / h
-            out = A * y0 + B * y1 + ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h) / 6.0
+            if x.dtype == np.float32:
+                # "... * (h * h) / 6.0": the quotient and the final sum in
+                # double, one rounding to REAL_T at the store
+                num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h)
+                out = ((A * y0 + B * y1).astype(np.float64)
+                       + num.astype(np.float64) / 6.0).astype(np.float32)
+            else:
+                out = A * y0 + B * y1 + ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h) / 6.0
     return out, in_range
 
 
@@ -466,15 +511,18 @@ def check_imf(imf_new: np.ndarray, imf_old: np.ndarray, any_bad_sign: bool,
         std_sum = lane_sum(q * q, lanes)
         old_max = lane_max(imf_old)
         old_min = lane_min(imf_old)
-        if sum_new_sq < SUM_NEW_SQ_MIN:
+        R = imf_new.dtype.type
+        # double literal: compared in double (kernels.py:814)
+        if float(sum_new_sq) < SUM_NEW_SQ_MIN:
             return False
+        # the thresholds are REAL_T functions (kernels.py:81-85)
         svar = diff_sq_sum / (old_max - old_min)
-        if svar < SVAR_THR:
+        if svar < R(SVAR_THR):
             return True
-        if std_sum < STD_THR:
+        if std_sum < R(STD_THR):
             return True
         energy_ratio = diff_sq_sum / old_sq_sum
-        if energy_ratio < ENERGY_RATIO_THR:
+        if energy_ratio < R(ENERGY_RATIO_THR):
             return True
     return False
 
@@ -486,12 +534,13 @@ def check_imf(imf_new: np.ndarray, imf_old: np.ndarray, any_bad_sign: bool,
 def emd_signal(S: np.ndarray, T: np.ndarray, cfg: OracleConfig | None = None,
                collect_stats: bool = False) -> SignalResult:
     cfg = cfg or OracleConfig()
-    S = np.ascontiguousarray(S, dtype=np.float64)
-    T = np.ascontiguousarray(T, dtype=np.float64)
+    R = cfg.rtype
+    S = np.ascontiguousarray(S, dtype=R)
+    T = np.ascontiguousarray(T, dtype=R)
     N = S.shape[0]
     lanes = cfg.threads_per_block
     MAXI = cfg.max_imfs
-    imfs = np.zeros((MAXI, N))
+    imfs = np.zeros((MAXI, N), dtype=R)
     dbg_n = np.full(MAXI, -1, dtype=np.int32)
     dbg_e = np.full(MAXI, -1, dtype=np.int32)
     dbg_z = np.full(MAXI, -1, dtype=np.int32)
@@ -565,14 +614,14 @@ def emd_signal(S: np.ndarray, T: np.ndarray, cfg: OracleConfig | None = None,
         gmax = lane_max(residue)
         gmin = lane_min(residue)
         gabs = lane_sum(np.abs(residue), lanes)
-        if (gmax - gmin) < RANGE_THR or gabs < TOTAL_POWER_THR:
+        if (gmax - gmin) < R(RANGE_THR) or gabs < R(TOTAL_POWER_THR):
             finished = True
 
     if extNo_last <= 2 and imf_count > 0:
         imf_count -= 1
         residue = residue + imf
-    absmax = float(np.fmax.reduce(np.abs(residue), initial=0.0))
-    residue_is_zero = absmax <= RESIDUE_ZERO_ATOL
+    absmax = float(np.fmax.reduce(np.abs(residue), initial=R(0.0)))
+    residue_is_zero = absmax <= RESIDUE_ZERO_ATOL      # double literal: compared in double
     if not residue_is_zero:
         imfs[imf_count] = residue
     n_imfs = imf_count if residue_is_zero else imf_count + 1

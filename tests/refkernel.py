@@ -20,6 +20,15 @@ def have_ref(name: str = "libemd_ref.so") -> bool:
     return os.path.isfile(ref_lib_path(name))
 
 
+def f32_name(name: str) -> str:
+    """The REAL_T = float build of a reference variant:
+    libemd_ref[_small][_nofma].so -> libemd_ref[_small]_f32[_nofma].so."""
+    stem = name[:-3]
+    if stem.endswith("_nofma"):
+        return stem[:-6] + "_f32_nofma.so"
+    return stem + "_f32.so"
+
+
 class RefKernel:
     """ctypes handle on one reference build variant."""
 
@@ -34,15 +43,24 @@ class RefKernel:
         cfg = (ctypes.c_int * 5)()
         self.lib.ref_config(cfg)
         self.max_extrema, self.nbsym, self.max_iteration, self.max_imfs, self.threads = list(cfg)
+        # REAL_T of the build (4: float); builds that predate the query are double
+        nbytes = self.lib.ref_real_bytes() if hasattr(self.lib, "ref_real_bytes") else 8
+        self.np_dtype = np.float32 if nbytes == 4 else np.float64
+
+    @property
+    def torch_dtype(self):
+        import torch
+        return torch.float32 if self.np_dtype == np.float32 else torch.float64
 
     def run_device(self, sig, T, stream=None):
-        """sig [B,N] f64 cuda, T [N] f64 cuda -> the reference's 6-tuple
+        """sig [B,N] REAL_T cuda, T [N] REAL_T cuda -> the reference's 6-tuple
         (kernels.py:1343-1372), allocated and zero/−1-filled like run()."""
         import torch
         B, N = sig.shape
         dev = sig.device
-        pools = torch.empty(6 * B * N, dtype=torch.float64, device=dev)
-        imfs = torch.zeros((B, self.max_imfs, N), dtype=torch.float64, device=dev)
+        rt = self.torch_dtype
+        pools = torch.empty(6 * B * N, dtype=rt, device=dev)
+        imfs = torch.zeros((B, self.max_imfs, N), dtype=rt, device=dev)
         n_imfs = torch.zeros(B, dtype=torch.int32, device=dev)
         ovf = torch.zeros(B, dtype=torch.int32, device=dev)
         dn = torch.full((B, self.max_imfs), -1, dtype=torch.int32, device=dev)
@@ -58,8 +76,8 @@ class RefKernel:
 
     def run(self, signals: np.ndarray, T: np.ndarray):
         import torch
-        sig = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float64)).cuda()
-        Td = torch.from_numpy(np.ascontiguousarray(T, dtype=np.float64)).cuda()
+        sig = torch.from_numpy(np.ascontiguousarray(signals, dtype=self.np_dtype)).cuda()
+        Td = torch.from_numpy(np.ascontiguousarray(T, dtype=self.np_dtype)).cuda()
         out = self.run_device(sig, Td)
         torch.cuda.synchronize()
         return tuple(o.cpu().numpy() for o in out)
@@ -67,11 +85,11 @@ class RefKernel:
     def envelope(self, signals: np.ndarray, T: np.ndarray):
         """run_envelope_only's 9-tuple (kernels.py:1374-1407)."""
         import torch
-        sig = torch.from_numpy(np.ascontiguousarray(signals, dtype=np.float64)).cuda()
-        Td = torch.from_numpy(np.ascontiguousarray(T, dtype=np.float64)).cuda()
+        sig = torch.from_numpy(np.ascontiguousarray(signals, dtype=self.np_dtype)).cuda()
+        Td = torch.from_numpy(np.ascontiguousarray(T, dtype=self.np_dtype)).cuda()
         B, N = sig.shape
         mbuf = self.max_extrema + 2 * self.nbsym
-        z = lambda *s, dt=torch.float64: torch.zeros(s, dtype=dt, device="cuda")
+        z = lambda *s, dt=self.torch_dtype: torch.zeros(s, dtype=dt, device="cuda")
         outs = [z(B, N), z(B, N), z(B, 2, dt=torch.int32), z(B, dt=torch.int32),
                 z(B, mbuf), z(B, mbuf), z(B, mbuf), z(B, mbuf), z(B, 2, dt=torch.int32)]
         rc = self.lib.ref_envelope_launch(sig.data_ptr(), Td.data_ptr(), B, N,

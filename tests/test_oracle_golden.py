@@ -83,3 +83,39 @@ def test_oracle_envelope_stage(golden):
         rng = float(np.ptp(X[b])) or 1.0
         assert np.max(np.abs(emax - golden[f"{name}__env__max_env"][b])) <= IMF_RTOL * rng
         assert np.max(np.abs(emin - golden[f"{name}__env__min_env"][b])) <= IMF_RTOL * rng
+
+
+# ---------------------------------------------------------------------------
+# REAL_T = float: the oracle in float32 against the reference source built
+# with REAL_T = float (tests/golden/ref_golden_f32.npz, make_golden.py --real
+# float).  Bit-identical to the -fmad=false build, equal discrete outputs.
+# ---------------------------------------------------------------------------
+
+def _sha32(block):
+    return hashlib.sha256(np.ascontiguousarray(block, dtype="<f4").tobytes()).hexdigest().encode()
+
+
+@pytest.fixture(scope="module")
+def golden32():
+    import os
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                "ref_golden_f32.npz"))
+
+
+@pytest.mark.parametrize("name", GROUPS)
+def test_oracle_f32_matches_reference_f32(golden32, name):
+    X = golden32[f"{name}__signals"]
+    T = golden32[f"{name}__T"]
+    assert X.dtype == np.float32 and T.dtype == np.float32
+    c = golden32[f"{name}__cfg"]
+    cfg = O.OracleConfig(max_extrema=int(c[0]), nbsym=int(c[1]), max_iteration=int(c[2]),
+                         max_imfs=int(c[3]), threads_per_block=int(c[4]), real_t="float")
+    for b in range(X.shape[0]):
+        r = O.emd_signal(X[b], T, cfg)
+        assert r.imfs.dtype == np.float32
+        assert r.n_imfs == golden32[f"{name}__nofma__n_imfs"][b], (name, b)
+        assert r.overflow == golden32[f"{name}__nofma__overflow"][b], (name, b)
+        np.testing.assert_array_equal(r.debug_n, golden32[f"{name}__nofma__dbg_n"][b])
+        np.testing.assert_array_equal(r.debug_extno, golden32[f"{name}__nofma__dbg_ext"][b])
+        np.testing.assert_array_equal(r.debug_nzm, golden32[f"{name}__nofma__dbg_nzm"][b])
+        assert _sha32(r.imfs) == golden32[f"{name}__nofma__sha"][b], (name, b, "bit-exact")
