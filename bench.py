@@ -380,7 +380,7 @@ def main():
         emd_tr = GPUBatchEMD(dataclasses.replace(cfg, real_t="double")) if f32 else emd
         ltr = emd_tr._get_launcher()
         otr = ltr.run(xtr, None)
-        cm = S.CostModel(dev, seed=0)
+        cm = S.CostModel(local, seed=0)
         cm.fit(S.features(xtr), S.labels_from_debug(otr[3], otr[1]), epochs=30, batch=256)
         cm.warmup()
         del otr, xtr
