@@ -176,13 +176,16 @@ constexpr int kPhases = 10;
 // their C++ meaning, so float expressions that mix them are evaluated in
 // double and rounded once, as in the reference source compiled with REAL_T =
 // float.  The FP64 build's division shortcuts (reciprocal tables, Markstein
-// and branch-free quotients) are off: float quotients are the IEEE ones.
+// and branch-free quotients) are off: float quotients are the IEEE ones, and
+// the one double quotient per envelope sample (the reference's "/ 6.0")
+// takes the Markstein quotient from RN(1/6) (EMDB_FAST_DIV 2), which equals
+// the double division.
 #ifndef EMDB_F32
 #define EMDB_F32 0
 #endif
 #if EMDB_F32
 #undef EMDB_FAST_DIV
-#define EMDB_FAST_DIV 0
+#define EMDB_FAST_DIV 2
 #undef EMDB_PCR_NB
 #define EMDB_PCR_NB 0
 namespace emdb::f32 {
@@ -1167,7 +1170,6 @@ __device__ __forceinline__ real eval_seg(const SideView& s, real t, int lo) {
 // eval_seg with the quotients taken from reciprocals (EMDB_FAST_DIV 1..3), in
 // the same operation order; sets `slow` when a quotient needs the division,
 // and the caller then re-evaluates the sample with eval_seg.
-#if !EMDB_F32
 __device__ __forceinline__ real eval_seg_q(const SideView& s, real t, int lo, bool& slow) {
   if (s.n < 4) return EMDB_EVAL_RARE(s, t, lo);
   const real* x = s.x;
@@ -1191,7 +1193,6 @@ __device__ __forceinline__ real eval_seg_q(const SideView& s, real t, int lo, bo
   real num = ((A * A * A - A) * M0 + (B * B * B - B) * M1) * (h * h);
   return (A * y0 + B * y1) + div_q(num, 6.0, kInv6, slow);
 }
-#endif
 
 // The reference's per-sample binary search (kernels.py:722-726).
 __device__ __forceinline__ int search_seg(const SideView& s, real t) {
@@ -1489,6 +1490,9 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
 #if EMDB_FAST_DIV
     bool slow = false;
     real emax, emin, emax2 = 0.0, emin2 = 0.0;
+#if !EMDB_F32
+    // (the FP32 build has no integer-axis shortcut: a float quotient formed
+    // in double from the table's RN(1/h) would be rounded twice)
     if (kInt) {
       emax = eval_seg_int(sv0, t, lo0, slow, fast);
       emin = eval_seg_int(sv1, t, lo1, slow, fast);
@@ -1496,7 +1500,9 @@ __device__ __forceinline__ int sift_pass(const SmemLayout& L, char* slab, const 
         emax2 = eval_seg_int(sv0, t2, lo0b, slow, fast);
         emin2 = eval_seg_int(sv1, t2, lo1b, slow, fast);
       }
-    } else {
+    } else
+#endif
+    {
       emax = eval_seg_q(sv0, t, lo0, slow);
       emin = eval_seg_q(sv1, t, lo1, slow);
       if (has2) {
