@@ -255,6 +255,8 @@ def main():
                     help="dense workloads: queue order of the timed steps (learned: the cost "
                          "model, trained here on a disjoint seeded batch, orders each step's "
                          "queue longest-predicted-first; the FIFO rate is reported beside it)")
+    ap.add_argument("--order-train", type=int, default=4,
+                    help="--order learned: seeded batches of the workload to train on")
     ap.add_argument("--train-traces", type=int, default=200000, help="ragged64k: MLP training set")
     ap.add_argument("--eval-traces", type=int, default=0, help="ragged64k: batch size (0 = 65536)")
     ap.add_argument("--epochs", type=int, default=20)
@@ -375,15 +377,21 @@ def main():
     if a.order == "learned":
         from cuda_emd import scheduler as S
         t_tr = time.perf_counter()
-        Xtr = make_workload(a.workload, rank + 1000)         # same generator, disjoint seed
-        xtr = torch.from_numpy(Xtr).to(dev)
         emd_tr = GPUBatchEMD(dataclasses.replace(cfg, real_t="double")) if f32 else emd
         ltr = emd_tr._get_launcher()
-        otr = ltr.run(xtr, None)
+        feats, labels, n_tr = [], [], 0
+        for k in range(a.order_train):
+            # same generator, seeds disjoint from the timed batch's
+            xtr = torch.from_numpy(make_workload(a.workload, rank + 1000 * (k + 1))).to(dev)
+            otr = ltr.run(xtr, None)
+            feats.append(S.features(xtr))
+            labels.append(S.labels_from_debug(otr[3], otr[1]))
+            n_tr += xtr.shape[0]
+            del otr, xtr
         cm = S.CostModel(local, seed=0)
-        cm.fit(S.features(xtr), S.labels_from_debug(otr[3], otr[1]), epochs=30, batch=256)
+        cm.fit(torch.cat(feats), torch.cat(labels), epochs=a.epochs, batch=256)
         cm.warmup()
-        del otr, xtr
+        del feats, labels
         torch.cuda.synchronize(dev)
         train_s = time.perf_counter() - t_tr
 
@@ -420,8 +428,8 @@ def main():
                    "speedup_learned": round(elapsed / el_learned, 4),
                    "true_cost_ms_per_step": round(el_true / a.steps * 1e3, 3),
                    "speedup_true_cost": round(elapsed / el_true, 4),
-                   "train": f"{Xtr.shape[0]} traces of the same generator (disjoint seed), "
-                            f"30 epochs, {train_s:.1f} s",
+                   "train": f"{n_tr} traces of the same generator (disjoint seeds), "
+                            f"{a.epochs} epochs, {train_s:.1f} s",
                    "note": "learned step = features + BF16 inference + LPT order + the launch, "
                            "all inside the timed region; true-cost = the queue ordered by the "
                            "logged sift passes (known only afterwards): the ordering ceiling",
