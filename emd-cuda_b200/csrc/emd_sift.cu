@@ -184,10 +184,17 @@ constexpr int kPhases = 10;
 #define EMDB_F32 0
 #endif
 #if EMDB_F32
+//  EMDB_F32_FAST  the float counterparts of the FP64 build's branch-free
+//                  quotients (div_q from an IEEE reciprocal for the segment
+//                  quotients, div_nb for the PCR rows), self-tested against
+//                  the float division by emdb_check_division modes 3 and 4
+#ifndef EMDB_F32_FAST
+#define EMDB_F32_FAST 1
+#endif
 #undef EMDB_FAST_DIV
-#define EMDB_FAST_DIV 2
+#define EMDB_FAST_DIV (EMDB_F32_FAST ? 3 : 2)
 #undef EMDB_PCR_NB
-#define EMDB_PCR_NB 0
+#define EMDB_PCR_NB EMDB_F32_FAST
 namespace emdb::f32 {
 using real = float;
 #else
@@ -519,6 +526,50 @@ __host__ __device__ inline int choose_place(int N, int arena_bytes, size_t slab_
 // outside that range, so a caller can redo a whole sample with the division
 // once instead of branching on every quotient.
 __device__ __noinline__ double div_slow(double a, double b) { return a / b; }
+
+#if EMDB_F32
+// Float counterparts (same methods, binary32 ranges): div_q is the two-step
+// Markstein quotient from y = RN(1/b); div_nb the branch-free quotient from
+// the approximate reciprocal (one Newton step reaches binary32 accuracy), a
+// faithful quotient and the exact-remainder choice of its neighbour (Muller
+// et al., Handbook of Floating-Point Arithmetic, ch. 4.9 / 5.3).  `slow` is
+// set outside the ranges where every step is exact: |a|, |q| in
+// (2^-100, 2^100), |b| in (2^-110, 2^110).
+__device__ __noinline__ float div_slow(float a, float b) { return a / b; }
+
+__device__ __forceinline__ float div_q(float a, float b, float y, bool& slow) {
+  const float q0 = a * y;
+  const float e0 = fmaf(-q0, b, a);
+  const float q1 = fmaf(e0, y, q0);
+  const float e1 = fmaf(-q1, b, a);
+  const float q2 = fmaf(e1, y, q1);
+  const float aa = fabsf(a), qa = fabsf(q0);
+  const bool zero = a == 0.0f;
+  slow |= !(zero || (aa > 0x1p-100f && aa < 0x1p+100f && qa > 0x1p-100f && qa < 0x1p+100f));
+  return zero ? q0 : q2;
+}
+
+__device__ __forceinline__ float div_nb(float a, float b, bool& slow) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+  const float e = fmaf(-b, y, 1.0f);
+  y = fmaf(y, e, y);
+  const float q0 = a * y;
+  const float r0 = fmaf(-q0, b, a);
+  const float q1 = fmaf(r0, y, q0);
+  const float r1 = fmaf(-q1, b, a);
+  const bool up = (r1 > 0.0f) == (b > 0.0f);
+  const int step = (up == (q1 > 0.0f)) ? 1 : -1;
+  const float qn = __int_as_float(__float_as_int(q1) + step);
+  const float rn = fmaf(-qn, b, a);
+  const float q = fabsf(rn) < fabsf(r1) ? qn : q1;
+  const float aa = fabsf(a), qa = fabsf(q1), ba = fabsf(b);
+  const bool bok = ba > 0x1p-110f && ba < 0x1p+110f;
+  const bool zero = a == 0.0f;
+  slow |= !bok || (!zero && !(aa > 0x1p-100f && aa < 0x1p+100f && qa > 0x1p-100f && qa < 0x1p+100f));
+  return zero ? q0 : q;
+}
+#endif
 
 // Rarely taken paths of the hot loops (fewer than 4 knots, operands outside
 // the fast quotients' range, knot lists that are not strictly increasing) as
@@ -1185,7 +1236,7 @@ __device__ __forceinline__ real eval_seg_q(const SideView& s, real t, int lo, bo
 #if EMDB_FAST_DIV == 1
   real rh = s.R[lo];
 #else
-  real rh = 1.0 / h;
+  const real rh = real(1) / h;
 #endif
   real A = div_q(x1 - t, h, rh, slow);
   real B = div_q(t - x0, h, rh, slow);
@@ -2105,6 +2156,87 @@ __global__ void div_check_kernel(int mode, long long n, unsigned long long seed,
 cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
                              unsigned long long* mismatches, cudaStream_t stream) {
   div_check_kernel<<<148 * 8, 256, 0, stream>>>(mode, n, seed, mismatches);
+  return cudaGetLastError();
+}
+#endif
+
+#if EMDB_F32
+// ---------------------------------------------------------------------------
+// Self-test of the float quotients (div_q, div_nb above) against the float
+// division.  mode 0: every integer pair 0 <= a <= b <= n through div_q with
+// y = RN(1/b) (the segment quotients on the default time axis); mode 1: n
+// pseudo-random pairs, [0] div_q with y = RN(1/b), significands random and
+// exponents in [-40, 40]; [1] div_nb with exponents in [-140, 140] (zeros,
+// subnormals and the range edges through the fallback); [2] div_nb on
+// PCR-like rows, |a| <= |b| within 2^+-40 of 1.  Counts mismatching bits.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64f(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ float rnd_float(uint64_t h, int e_lo, int e_hi) {
+  const float m = __int_as_float((int)((h >> 41) | 0x3f800000u));     // [1, 2)
+  const float v = ldexpf(m, (int)(h % (uint64_t)(e_hi - e_lo + 1)) + e_lo);
+  return (h & (1ull << 20)) ? -v : v;
+}
+
+__global__ void div_check_f32_kernel(int mode, long long n, unsigned long long seed,
+                                     unsigned long long* mismatches) {
+  unsigned long long bad0 = 0, bad1 = 0, bad2 = 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (mode == 0) {
+    for (long long bb = 1 + blockIdx.x * (long long)blockDim.x + threadIdx.x; bb <= n; bb += stride) {
+      const float b = (float)bb;
+      const float y = 1.0f / b;
+      for (long long aa = 0; aa <= bb; ++aa) {
+        const float a = (float)aa;
+        bool slow = false;
+        float q = div_q(a, b, y, slow);
+        if (slow) q = div_slow(a, b);
+        if (__float_as_int(q) != __float_as_int(div_slow(a, b))) ++bad0;
+      }
+    }
+  } else {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+      const uint64_t h1 = mix64f(seed ^ (uint64_t)i), h2 = mix64f(h1 ^ 0x5bd1e995ull);
+      const uint64_t h3 = mix64f(h2 ^ 0x9e3779b9ull), h4 = mix64f(h3 ^ 0x7f4a7c15ull);
+      {
+        const float a = rnd_float(h1, -40, 40), b = rnd_float(h2, -40, 40);
+        bool slow = false;
+        float q = div_q(a, b, 1.0f / b, slow);
+        if (slow) q = div_slow(a, b);
+        if (__float_as_int(q) != __float_as_int(div_slow(a, b))) ++bad0;
+      }
+      {
+        float a = rnd_float(h3, -140, 140), b = rnd_float(h4, -140, 140);
+        if ((h3 & 0xff) == 0) a = 0.0f;
+        bool slow = false;
+        float q = div_nb(a, b, slow);
+        if (slow) q = div_slow(a, b);
+        if (__float_as_int(q) != __float_as_int(div_slow(a, b))) ++bad1;
+      }
+      {
+        const float b = rnd_float(h2 ^ h3, -40, 40);
+        const float f = __int_as_float((int)((h4 >> 41) | 0x3f800000u)) - 1.0f;   // [0, 1)
+        const float a = ((h1 & 2) ? -f : f) * b;
+        bool slow = false;
+        float q = div_nb(a, b, slow);
+        if (slow) q = div_slow(a, b);
+        if (__float_as_int(q) != __float_as_int(div_slow(a, b))) ++bad2;
+      }
+    }
+  }
+  if (bad0) atomicAdd(mismatches, bad0);
+  if (bad1) atomicAdd(mismatches + 1, bad1);
+  if (bad2) atomicAdd(mismatches + 2, bad2);
+}
+
+cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
+                             unsigned long long* mismatches, cudaStream_t stream) {
+  div_check_f32_kernel<<<148 * 8, 256, 0, stream>>>(mode, n, seed, mismatches);
   return cudaGetLastError();
 }
 #endif

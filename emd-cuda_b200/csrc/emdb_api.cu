@@ -1041,13 +1041,15 @@ __attribute__((visibility("hidden"))) int emdb_noalloc_auto_arena(int smem_optin
 
 int emdb_check_division(int mode, long long n, unsigned long long seed,
                         unsigned long long* mismatches) {
-  if (!mismatches || mode < 0 || mode > 2 || n < 0)
+  if (!mismatches || mode < 0 || mode > 4 || n < 0)
     return fail(EMDB_ERR_INVALID, "bad self-test arguments");
   unsigned long long* d = nullptr;
   cudaError_t e = cudaMalloc(&d, 3 * sizeof(unsigned long long));
   if (e != cudaSuccess) return cuda_fail(e, "self-test counter");
   e = cudaMemset(d, 0, 3 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = emdb::launch_div_check(mode, n, seed, d, 0);
+  if (e == cudaSuccess)
+    e = mode >= 3 ? emdb::f32::launch_div_check(mode - 3, n, seed, d, 0)
+                  : emdb::launch_div_check(mode, n, seed, d, 0);
   if (e == cudaSuccess)
     e = cudaMemcpy(mismatches, d, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
   cudaFree(d);

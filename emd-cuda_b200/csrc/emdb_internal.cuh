@@ -140,6 +140,8 @@ cudaError_t launch_envelope(const EnvParams& p, int grid, cudaStream_t stream);
 cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm,
                            bool imf_global = false);
 cudaError_t envelope_occupancy(int arena_bytes, int* ctas_per_sm);
+cudaError_t launch_div_check(int mode, long long n, unsigned long long seed,
+                             unsigned long long* mismatches, cudaStream_t stream);
 }  // namespace f32
 
 }  // namespace emdb

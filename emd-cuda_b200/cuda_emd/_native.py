@@ -251,6 +251,7 @@ def check_division(mode: int, n: int, seed: int = 0) -> tuple[int, int, int]:
     """Self-test: mismatches of the kernels' own divisions vs the hardware
     division, three counters per mode (mode 0/1: the reciprocal-based
     division of the evaluation; mode 2: the PCR rows' branch-free division;
+    modes 3/4: the FP32 kernels' float quotients against the float division;
     the header documents the cases)."""
     L = load()
     out = (ctypes.c_ulonglong * 3)()

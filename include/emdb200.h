@@ -313,7 +313,13 @@ int emdb_mlp_infer_bf16(const uint16_t* params_bf16, const float* X, const float
  * rows use (no reciprocal at hand), n seeded cases each of [0] a/b over
  * [2^-1100, 2^1100] (zeros, subnormals and infinities through its fallback),
  * [1] denominators with all-ones or power-of-two significands, [2] |a| <= |b|
- * within 2^+-40 of 1.  Synchronous on the current device. */
+ * within 2^+-40 of 1.  Modes 3 and 4: the FP32 kernels' float quotients
+ * against the float division -- mode 3 every integer pair 0 <= a <= b <= n
+ * through the reciprocal-based quotient; mode 4 n seeded cases each of [0]
+ * the reciprocal-based quotient over [2^-40, 2^40], [1] the branch-free
+ * quotient over [2^-140, 2^140] (zeros, subnormals, range edges through its
+ * fallback), [2] PCR-like |a| <= |b| within 2^+-40 of 1.  Synchronous on the
+ * current device. */
 int emdb_check_division(int mode, long long n, unsigned long long seed,
                         unsigned long long* mismatches);
 
