@@ -1694,7 +1694,10 @@ __device__ __forceinline__ void mark_trace_done(const SiftParams& p, int b, int 
 // 65536 / (NT * kMinBlocks) registers so that many CTAs can be resident.
 // kGImf (wide only): the proto-IMF in the global slab, for traces longer than
 // shared memory holds.
-template <int NT, int kMinBlocks, bool kInt, bool kGImf = false>
+// kTail: the build that takes part in tail migration -- a 128/256-thread
+// instance that hands its last traces over, or the 512-thread instance that
+// resumes them (p.resume).  The other builds carry none of its code.
+template <int NT, int kMinBlocks, bool kInt, bool kGImf = false, bool kTail = false>
 __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) {
   constexpr bool kWide = NT > kThreads;
   static_assert(!kGImf || kWide, "the global proto-IMF is built for the wide instance");
@@ -1710,12 +1713,26 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
   real* qbuf = kWide ? reinterpret_cast<real*>(slab + p.q_off) : nullptr;
   real* gimf = kGImf ? reinterpret_cast<real*>(slab + p.imf_off) : nullptr;
 
+  // this launch may hand over its tail / resumes another launch's tail
+  const bool migrate = kTail && !kWide && p.cont_buf != nullptr;
+  const bool resume = kTail && kWide && p.resume != 0;
   for (;;) {
-    if (tid == 0) Cs->job = atomicAdd(p.queue, 1);
+    if (tid == 0) Cs->job = atomicAdd(resume ? p.cont_ticket : p.queue, 1);
     __syncthreads();
     const int job = Cs->job;
-    if (job >= p.batch) break;
-    const int b = p.order ? p.order[job] : job;
+    // a resume launch takes the continuation records instead of the queue
+    const ContHead* rec = nullptr;
+    if (resume) {
+      if (job >= p.cont_cap) break;
+      if (!p.cont_valid[job]) {
+        __syncthreads();          // every thread has read Cs->job before it is reused
+        continue;
+      }
+      rec = reinterpret_cast<const ContHead*>(p.cont_buf + (size_t)job * p.cont_stride);
+    } else if (job >= p.batch) {
+      break;
+    }
+    const int b = rec ? rec->b : p.order ? p.order[job] : job;
     const int64_t off = p.offsets ? p.offsets[b] : (int64_t)b * p.dense_n;
     const int N = p.offsets ? (int)(p.offsets[b + 1] - off) : p.dense_n;
     const real* S = p.values + off;
@@ -1745,11 +1762,22 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     SmemLayout L = carve<NT, kGImf>(smem, N, p.arena_bytes, gimf);
     Ctl& C = *L.ctl;
     real* imf = L.imf;
-    for (int k = tid; k < MAXI; k += NT) { C.dbg_n[k] = -1; C.dbg_e[k] = -1; C.dbg_z[k] = -1; }
+    if (migrate && tid == 0) atomicAdd(p.active, 1);
+    for (int k = tid; k < MAXI; k += NT) {
+      C.dbg_n[k] = rec ? rec->dbg[0][k] : -1;
+      C.dbg_e[k] = rec ? rec->dbg[1][k] : -1;
+      C.dbg_z[k] = rec ? rec->dbg[2][k] : -1;
+    }
 #if EMDB_LOAD_CLOCKS
     const long long clk_trace0 = clock64();
 #endif
-    for (int i = tid; i < N; i += NT) imf[i] = S[i];
+    {
+      // a resumed trace restarts from its parked proto-IMF
+      const real* src = rec ? reinterpret_cast<const real*>(reinterpret_cast<const char*>(rec) +
+                                                          cont_data_off())
+                            : S;
+      for (int i = tid; i < N; i += NT) imf[i] = src[i];
+    }
     __syncthreads();
 #if EMDB_LOAD_CLOCKS
     if (tid == 0 && p.counters)
@@ -1760,19 +1788,36 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
     }
 #endif
 
-    bool ovf = false;
-    int imf_count = 0;
+    bool ovf = rec ? rec->ovf != 0 : false;
+    int imf_count = rec ? rec->imf_count : 0;
     bool finished = false;
-    int extNo_last = -1;
-    bool stale = false;
+    int extNo_last = rec ? rec->extNo_last : -1;
+    bool stale = rec ? rec->stale != 0 : false;
+    int n_resume = rec ? rec->n : 0;
+    bool yielded = false;
+    int n_yield = 0;
     unsigned long long passes = 0, spilled = 0;
 
     ExtInfo e = extrema_scan<NT>(L, N, tid, warp, lane, p.max_extrema);
     ovf |= e.overflow;
 
     while (!finished && imf_count < MAXI - 1) {
-      int n = 0;
+      int n = n_resume;
+      n_resume = 0;
       for (;;) {
+        if (migrate) {
+          // every trace has started and few remain: hand this one to the
+          // 512-thread instance at this pass boundary
+          int want = 0;
+          if (tid == 0)
+            want = *reinterpret_cast<volatile int*>(p.queue) >= p.batch &&
+                   *reinterpret_cast<volatile int*>(p.active) <= p.yield_below;
+          if (__syncthreads_or(want)) {
+            yielded = true;
+            n_yield = n;
+            break;
+          }
+        }
         ++n;
         if (n >= p.max_iteration) {
           ovf = true;
@@ -1856,6 +1901,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
           break;
         }
       }
+      if (yielded) break;
       // ---- emit IMF row, running residue into the next row, end condition ----
       EMDB_PH(&C, 9);
       {
@@ -1895,6 +1941,35 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         ovf |= e.overflow;
       }
       EMDB_PH(&C, 8);
+    }
+
+    if (yielded) {
+      // continuation record in this CTA's slot (a CTA hands over at most one
+      // trace: the queue is empty when it does)
+      ContHead* h = reinterpret_cast<ContHead*>(p.cont_buf + (size_t)blockIdx.x * p.cont_stride);
+      real* dst = reinterpret_cast<real*>(reinterpret_cast<char*>(h) + cont_data_off());
+      for (int i = tid; i < N; i += NT) dst[i] = imf[i];
+      for (int k = tid; k < kMaxImfsCap; k += NT) {
+        h->dbg[0][k] = C.dbg_n[k];
+        h->dbg[1][k] = C.dbg_e[k];
+        h->dbg[2][k] = C.dbg_z[k];
+      }
+      if (tid == 0) {
+        h->b = b;
+        h->n = n_yield;
+        h->imf_count = imf_count;
+        h->extNo_last = extNo_last;
+        h->ovf = ovf ? 1 : 0;
+        h->stale = stale ? 1 : 0;
+        p.cont_valid[blockIdx.x] = 1;
+        atomicSub(p.active, 1);
+        if (p.counters) {
+          atomicAdd(p.counters, passes);
+          atomicAdd(p.counters + 1, spilled);
+        }
+      }
+      __syncthreads();
+      continue;
     }
 
     // ---- epilogue: trend removal, residue ~ 0 test, zero unused rows ----
@@ -1937,6 +2012,7 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
         atomicAdd(p.counters, passes);
         atomicAdd(p.counters + 1, spilled);
       }
+      if (migrate) atomicSub(p.active, 1);
     }
     if (stale) atomicOr(p.status, kStatusStaleEnvelope);
     for (int k = tid; k < MAXI; k += NT) {
@@ -2283,18 +2359,18 @@ cudaError_t occupancy_v(int arena_bytes, int* ctas_per_sm) {
   *ctas_per_sm = a < b ? a : b;
   return e;
 }
-template <int NT, int V, bool kInt, bool kG = false>
+template <int NT, int V, bool kInt, bool kG = false, bool kT = false>
 cudaError_t launch_vt(const SiftParams& p, int grid, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<NT, V, kInt, kG>,
+  cudaError_t e = cudaFuncSetAttribute(emd_sift_kernel<NT, V, kInt, kG, kT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, p.arena_bytes);
   if (e != cudaSuccess) return e;
-  emd_sift_kernel<NT, V, kInt, kG><<<grid, NT, p.arena_bytes, stream>>>(p);
+  emd_sift_kernel<NT, V, kInt, kG, kT><<<grid, NT, p.arena_bytes, stream>>>(p);
   return cudaGetLastError();
 }
-template <int NT, int V, bool kG = false>
+template <int NT, int V, bool kG = false, bool kT = false>
 cudaError_t launch_v(const SiftParams& p, int grid, cudaStream_t stream) {
-  return p.t_mode == kTArange ? launch_vt<NT, V, true, kG>(p, grid, stream)
-                              : launch_vt<NT, V, false, kG>(p, grid, stream);
+  return p.t_mode == kTArange ? launch_vt<NT, V, true, kG, kT>(p, grid, stream)
+                              : launch_vt<NT, V, false, kG, kT>(p, grid, stream);
 }
 }  // namespace
 
@@ -2318,6 +2394,16 @@ cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm, bool 
 }
 
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream) {
+  // tail migration (p.cont_buf): the 128 x 4 and 256 x 2 builds that hand
+  // over, the 512-thread build that resumes
+  if (p.cont_buf != nullptr) {
+    switch (p.variant) {
+      case 1: return launch_v<kWideThreads, 1, false, true>(p, grid, stream);
+      case 2: return launch_v<kHalfWideThreads, 2, false, true>(p, grid, stream);
+      case 4: return launch_v<kThreads, 4, false, true>(p, grid, stream);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   switch (p.variant) {
     case 1: return p.imf_off ? launch_v<kWideThreads, 1, true>(p, grid, stream)
                              : launch_v<kWideThreads, 1>(p, grid, stream);

@@ -26,6 +26,12 @@ struct emdb_plan {
   int arena_override = 0;
   int variant = 0;            // kernel instance (register variant); 0 = by trace length
   int max_ctas = 0;           // cap on a launch's persistent grid (0 = resident CTAs)
+  int tail = -1;              // tail migration: 0 off, -1 below the SM count, > 0 that many
+  int* d_tail = nullptr;      // [0] traces in flight, [1] resume tickets
+  int* d_cont_valid = nullptr;
+  int cont_valid_cap = 0;
+  char* d_cont = nullptr;     // continuation records
+  size_t cont_bytes = 0;
   int* d_ctl = nullptr;       // [0] sift queue, [1] status, [2] envelope queue
   unsigned long long* d_cnt = nullptr;  // [0] sift passes, [1] spilled passes, [2] / [3]
                                         // load / trace cycles, [4..13] phase cycles
@@ -278,13 +284,16 @@ class ZeroRows {
 constexpr int kMaxTraceLen = 1 << 17;
 
 template <typename R>
-int prepare_sift(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, int* grid) {
+int prepare_sift(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, int* grid,
+                 int force_variant = 0) {
   using K = SiftKernels<R>;
   if (max_n > kMaxTraceLen)
     return fail(EMDB_ERR_UNSUPPORTED, "trace length " + std::to_string(max_n) +
                 " exceeds the longest supported trace (131072 samples)");
-  int variant = effective_variant(p, max_n);
-  int arena = arena_for<R>(p, max_n);
+  // force_variant: that instance at its automatic arena (the tail's resume launch)
+  int variant = force_variant ? force_variant : effective_variant(p, max_n);
+  int arena = force_variant ? auto_arena_for<R>(p->smem_optin, force_variant, p->cfg.nbsym, max_n)
+                            : arena_for<R>(p, max_n);
   bool gimf = false;
   if ((arena <= 0 || K::fixed_smem(max_n, variant) + 64 > (size_t)arena) &&
       p->arena_override == 0) {
@@ -333,19 +342,86 @@ int prepare_sift(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, i
   return EMDB_OK;
 }
 
+// Device buffers of tail migration for `grid` CTAs and traces up to max_n.
+template <typename R>
+int ensure_tail(emdb_plan* p, int grid, int max_n, size_t* stride) {
+  *stride = al256(emdb::cont_data_off() + (size_t)std::max(max_n, 1) * sizeof(R));
+  cudaError_t e = cudaSuccess;
+  if (!p->d_tail) e = cudaMalloc(&p->d_tail, 2 * sizeof(int));
+  if (e == cudaSuccess && grid > p->cont_valid_cap) {
+    if (p->d_cont_valid) cudaFree(p->d_cont_valid);
+    p->d_cont_valid = nullptr;
+    p->cont_valid_cap = 0;
+    e = cudaMalloc(&p->d_cont_valid, (size_t)grid * sizeof(int));
+    if (e == cudaSuccess) p->cont_valid_cap = grid;
+  }
+  const size_t bytes = *stride * (size_t)grid;
+  if (e == cudaSuccess && bytes > p->cont_bytes) {
+    if (p->d_cont) cudaFree(p->d_cont);
+    p->d_cont = nullptr;
+    p->cont_bytes = 0;
+    e = cudaMalloc(&p->d_cont, bytes);
+    if (e == cudaSuccess) p->cont_bytes = bytes;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "allocating the tail-migration records");
+  return EMDB_OK;
+}
+
 template <typename R = double>
 int launch_common(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, cudaStream_t st) {
   int grid = 0;
   int rc = prepare_sift<R>(p, sp, max_n, &grid);
   if (rc) return rc;
-  rc = ensure_slab(p, sp.slab_stride * (size_t)grid);
+  // tail migration: the traces still in flight when the queue runs dry move
+  // to a second launch of the 512-thread instance (not for launches of that
+  // instance already)
+  const bool tail = p->tail != 0 && (sp.variant == 4 || sp.variant == 2);
+  typename SiftKernels<R>::Params rp{};
+  int rgrid = 0;
+  size_t cont_stride = 0;
+  if (tail) {
+    rp = sp;
+    rc = prepare_sift<R>(p, rp, max_n, &rgrid, 1);
+    if (rc) return rc;
+    rgrid = std::min(rgrid, grid);
+    rc = ensure_tail<R>(p, grid, max_n, &cont_stride);
+    if (rc) return rc;
+  }
+  rc = ensure_slab(p, std::max(sp.slab_stride * (size_t)grid,
+                               tail ? rp.slab_stride * (size_t)rgrid : 0));
   if (rc) return rc;
   sp.queue = p->d_ctl;
   sp.slab = p->d_slab;
   cudaError_t e = cudaMemsetAsync(p->d_ctl, 0, sizeof(int), st);
   if (e != cudaSuccess) return cuda_fail(e, "queue reset");
+  if (tail) {
+    e = cudaMemsetAsync(p->d_tail, 0, 2 * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->d_cont_valid, 0, (size_t)grid * sizeof(int), st);
+    if (e != cudaSuccess) return cuda_fail(e, "tail reset");
+    sp.active = p->d_tail;
+    sp.cont_ticket = p->d_tail + 1;
+    sp.yield_below = p->tail < 0 ? p->num_sms : p->tail;
+    sp.cont_buf = p->d_cont;
+    sp.cont_stride = cont_stride;
+    sp.cont_valid = p->d_cont_valid;
+    sp.cont_cap = grid;
+    sp.resume = 0;
+  }
   e = SiftKernels<R>::launch(sp, grid, st);
   if (e != cudaSuccess) return cuda_fail(e, "sift launch");
+  if (tail) {
+    rp.queue = p->d_ctl;
+    rp.slab = p->d_slab;
+    rp.active = nullptr;
+    rp.cont_ticket = p->d_tail + 1;
+    rp.cont_buf = p->d_cont;
+    rp.cont_stride = cont_stride;
+    rp.cont_valid = p->d_cont_valid;
+    rp.cont_cap = grid;
+    rp.resume = 1;
+    e = SiftKernels<R>::launch(rp, rgrid, st);
+    if (e != cudaSuccess) return cuda_fail(e, "tail launch");
+  }
   return EMDB_OK;
 }
 
@@ -402,6 +478,9 @@ int emdb_plan_destroy(emdb_plan* p) {
   {
     DeviceGuard g(p->device);
     if (p->d_slab) cudaFree(p->d_slab);
+    if (p->d_tail) cudaFree(p->d_tail);
+    if (p->d_cont_valid) cudaFree(p->d_cont_valid);
+    if (p->d_cont) cudaFree(p->d_cont);
     if (p->d_ctl) cudaFree(p->d_ctl);
     if (p->d_cnt) cudaFree(p->d_cnt);
     if (p->d_stage) cudaFree(p->d_stage);
@@ -439,6 +518,14 @@ int emdb_plan_set_variant(emdb_plan* p, int min_ctas_per_sm) {
                 "(512-thread wide CTAs) or 0 (by trace length)");
   std::lock_guard<std::mutex> lk(p->mu);
   p->variant = min_ctas_per_sm;
+  return EMDB_OK;
+}
+
+int emdb_plan_set_tail(emdb_plan* p, int yield_below) {
+  if (!p) return fail(EMDB_ERR_INVALID, "plan is NULL");
+  if (yield_below < -1) return fail(EMDB_ERR_INVALID, "yield_below must be >= -1");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->tail = yield_below;
   return EMDB_OK;
 }
 

@@ -70,7 +70,34 @@ struct SiftParamsT {
   int variant;                // 4, 5, 6: 128-thread CTAs, register budget for that many per
                               // SM; 1: the 512-thread wide instance, one CTA per SM;
                               // 2: 256-thread CTAs, two per SM
+  // Tail migration (cont_buf NULL = off).  Once every trace of the launch
+  // has started and at most yield_below are still in flight, each of them
+  // stops at its next sift-pass boundary and leaves a continuation record
+  // (its proto-IMF and loop state) in the record of its CTA; a second launch
+  // of the 512-thread instance with resume = 1 finishes them, one per SM.
+  int* active;                // traces in flight in this launch (zeroed before it)
+  int yield_below;
+  char* cont_buf;             // cont_cap records of cont_stride bytes, one per CTA
+  size_t cont_stride;
+  int* cont_valid;            // [cont_cap]: 1 = record holds a trace (zeroed before it)
+  int cont_cap;
+  int* cont_ticket;           // the resume launch's ticket counter (zeroed before it)
+  int resume;
 };
+
+// Header of a continuation record; the proto-IMF follows at cont_data_off().
+struct ContHead {
+  int b;                      // trace index
+  int n;                      // sift passes done on the current IMF
+  int imf_count;
+  int extNo_last;
+  int ovf;
+  int stale;
+  int dbg[3][kMaxImfsCap];    // debug_n / debug_extno / debug_nzm so far
+};
+__host__ __device__ constexpr size_t cont_data_off() {
+  return (sizeof(ContHead) + 255) & ~size_t(255);
+}
 
 template <typename R>
 struct EnvParamsT {

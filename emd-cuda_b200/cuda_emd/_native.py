@@ -37,7 +37,7 @@ EXPORTS = ("emdb_version", "emdb_plan_create", "emdb_plan_destroy", "emdb_plan_s
            "emdb_notify_create", "emdb_notify_reset", "emdb_notify_destroy",
            "emdb_run_ragged_notify", "emdb_pass_placement", "emdb_noalloc_status",
            "emdb_pack_rows", "emdb_run_f32", "emdb_run_ragged_f32", "emdb_envelope_f32",
-           "emdb_plan_query_f32")
+           "emdb_plan_query_f32", "emdb_plan_set_tail")
 
 
 class EmdbConfig(ctypes.Structure):
@@ -70,6 +70,7 @@ def load() -> ctypes.CDLL:
         L.emdb_plan_set_arena.argtypes = [VP, I]
         L.emdb_plan_set_variant.argtypes = [VP, I]
         L.emdb_plan_set_max_ctas.argtypes = [VP, I]
+        L.emdb_plan_set_tail.argtypes = [VP, I]
         L.emdb_plan_phase_clocks.argtypes = [VP, P, I, I]
         L.emdb_plan_query.argtypes = [VP, I, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]
         L.emdb_run.argtypes = [VP, P, P, I, I, P, P, P, P, P, P, VP]
@@ -197,6 +198,11 @@ class Plan:
 
     def set_variant(self, min_ctas_per_sm: int) -> None:
         check(self.L.emdb_plan_set_variant(self.handle, int(min_ctas_per_sm)), "emdb_plan_set_variant")
+
+    def set_tail(self, yield_below: int) -> None:
+        """Tail migration (emdb_plan_set_tail): 0 off, -1 below the SM count,
+        > 0 below that many traces in flight."""
+        check(self.L.emdb_plan_set_tail(self.handle, int(yield_below)), "emdb_plan_set_tail")
 
     def set_max_ctas(self, max_ctas: int) -> None:
         check(self.L.emdb_plan_set_max_ctas(self.handle, int(max_ctas)), "emdb_plan_set_max_ctas")

@@ -83,6 +83,19 @@ int emdb_plan_set_variant(emdb_plan* plan, int min_ctas_per_sm);
  * wide launch on a share of the SMs this way.  No reference counterpart (its
  * grid is one CTA per signal, kernels.py:1366-1367). */
 int emdb_plan_set_max_ctas(emdb_plan* plan, int max_ctas);
+/* Tail migration for the plan's dense and ragged launches of the 128-thread
+ * (4 per SM) and 256-thread instances (no reference counterpart; its launch is one CTA per
+ * signal, kernels.py:1366-1367).  Once every trace of a launch has started
+ * and at most yield_below of them are still in flight, each stops at its
+ * next sift-pass boundary, parks its proto-IMF and loop state in a
+ * plan-owned record, and a second launch of the 512-thread instance finishes
+ * them, one trace per SM -- the last traces of a batch then run on a whole
+ * SM instead of a quarter of one.  Same results bit for bit.  yield_below:
+ * -1 = the device's SM count (the default), 0 = off, > 0 that many traces.
+ * Measured on B200 (dense seismic, 2048 samples): 4,096 traces 26.1 -> 22.3
+ * ms, 16,384 traces 68.4 -> 67.1 ms; in FP32, where a few traces sift to
+ * the iteration cap, 73.7 -> 34.4 ms and 114.1 -> 77.3 ms. */
+int emdb_plan_set_tail(emdb_plan* plan, int yield_below);
 /* Arena and CTAs/SM the plan would use for traces up to max_n. */
 int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
                     int* grid_max);
