@@ -1805,9 +1805,10 @@ __global__ void __launch_bounds__(NT, kMinBlocks) emd_sift_kernel(SiftParams p) 
       int n = n_resume;
       n_resume = 0;
       for (;;) {
-        if (migrate) {
+        if (migrate && (n & 3) == 0) {
           // every trace has started and few remain: hand this one to the
-          // 512-thread instance at this pass boundary
+          // 512-thread instance at this pass boundary (checked every fourth
+          // pass: the two L2 reads and the barrier cost ~1 % per pass)
           int want = 0;
           if (tid == 0)
             want = *reinterpret_cast<volatile int*>(p.queue) >= p.batch &&

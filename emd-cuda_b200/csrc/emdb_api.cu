@@ -400,7 +400,12 @@ int launch_common(emdb_plan* p, typename SiftKernels<R>::Params& sp, int max_n, 
     if (e != cudaSuccess) return cuda_fail(e, "tail reset");
     sp.active = p->d_tail;
     sp.cont_ticket = p->d_tail + 1;
-    sp.yield_below = p->tail < 0 ? p->num_sms : p->tail;
+    // automatic: three traces per SM -- the resume launch runs a trace
+    // ~2.5x faster on a whole SM than a 128-thread CTA does, so handing
+    // over pays once fewer than that remain (B200, cfg1 shape: 16,384
+    // traces 67.1 ms at 1 per SM, 66.7-66.9 at 3, 67.2 at 4; 4,096 traces
+    // 22.4 / 21.9 / 21.9 ms)
+    sp.yield_below = p->tail < 0 ? 3 * p->num_sms : p->tail;
     sp.cont_buf = p->d_cont;
     sp.cont_stride = cont_stride;
     sp.cont_valid = p->d_cont_valid;

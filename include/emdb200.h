@@ -91,10 +91,10 @@ int emdb_plan_set_max_ctas(emdb_plan* plan, int max_ctas);
  * plan-owned record, and a second launch of the 512-thread instance finishes
  * them, one trace per SM -- the last traces of a batch then run on a whole
  * SM instead of a quarter of one.  Same results bit for bit.  yield_below:
- * -1 = the device's SM count (the default), 0 = off, > 0 that many traces.
- * Measured on B200 (dense seismic, 2048 samples): 4,096 traces 26.1 -> 22.3
- * ms, 16,384 traces 68.4 -> 67.1 ms; in FP32, where a few traces sift to
- * the iteration cap, 73.7 -> 34.4 ms and 114.1 -> 77.3 ms. */
+ * -1 = three per SM of the device (the default), 0 = off, > 0 that many.
+ * Measured on B200 (dense seismic, 2048 samples): 4,096 traces 25.9 -> 21.9
+ * ms, 16,384 traces 68.0 -> 66.7 ms; in FP32, where a few traces sift to
+ * the iteration cap, 16,384 traces 114.0 -> 77.0 ms. */
 int emdb_plan_set_tail(emdb_plan* plan, int yield_below);
 /* Arena and CTAs/SM the plan would use for traces up to max_n. */
 int emdb_plan_query(emdb_plan* plan, int max_n, int* arena_bytes, int* ctas_per_sm,
