@@ -84,6 +84,11 @@ class Tier:
         self.idx = idx                      # trace indices (host, int64)
         self.max_n = 0
         self.plan = _native.Plan(cfg.to_c(), device)
+        # the tier launches share the GPU (forked streams, the learned split's
+        # capped wide launch beside the light one): no tail migration, whose
+        # whole-SM resume launch assumes a launch that owns the GPU (measured:
+        # the learned step fell from 2.07 to 2.64 s with it on)
+        self.plan.set_tail(0)
         self.arena = 0
         self.variant = 4
 
