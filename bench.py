@@ -544,7 +544,10 @@ def main():
                        "overflow_traces": ovf, "parallelism": f"replicas x{world}"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
             "order": ordered,
-            "gpu_launches": a.steps * (3 if ordered else 1),
+            # each dense launch of the 128/256-thread instances is a pair
+            # (tail migration's resume launch); learned steps add the
+            # feature and inference kernels
+            "gpu_launches": a.steps * ((2 if ctas_per_sm >= 2 else 1) + (2 if ordered else 0)),
         }
         print(json.dumps(line), flush=True)
     R.finish(world)
