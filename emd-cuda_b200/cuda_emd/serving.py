@@ -387,11 +387,9 @@ class EMDServer:
             variant, arena = self._tier_instance(e, in_flight)
             p.set_variant(variant)
             p.set_arena(arena)
-            # tail migration hands a launch's last traces to whole SMs: right
-            # while the server's traces in flight fit one per SM, not when
-            # other slots' launches share the GPU (whole-SM CTAs would crowd
-            # them out)
-            p.set_tail(-1 if in_flight <= self.num_sms else 0)
+            # the plan's tail migration stays on: a serving launch is small,
+            # so its traces move to whole SMs once its queue is empty -- the
+            # measured sweeps favour it at 70 % load and above
             _native.check(p.L.emdb_run_ragged_notify(
                 p.handle, vals.data_ptr(), offs.data_ptr(), int(cnt), int(e), None, 1,
                 order.data_ptr(), imfs.data_ptr(), n_imfs.data_ptr(), ovf.data_ptr(),
