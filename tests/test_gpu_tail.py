@@ -87,3 +87,51 @@ def test_tail_migration_ragged_per_trace_axes():
     ref = run(_launcher())
     _same(ref, run(_launcher(tail=-1)))
     _same(ref, run(_launcher(tail=1 << 30)))
+
+
+@pytest.mark.parametrize("real", ["double", "float"])
+def test_tail_migration_golden_groups(real):
+    # every parity group (zeros, plateaus, tiny traces, both caps, a
+    # non-uniform axis, the small config) with every trace handed over: the
+    # reference's bits (the -fmad=false fixtures), FP64 and FP32
+    import hashlib
+    import os
+    import cases
+    from cuda_emd import EMDKernelConfig
+    here = os.path.dirname(os.path.abspath(__file__))
+    z = np.load(os.path.join(here, "golden", "ref_golden_f32.npz" if real == "float"
+                             else "ref_golden.npz"))
+    code = "<f4" if real == "float" else "<f8"
+    for g in cases.groups():
+        name = g["name"]
+        X, T, c = z[f"{name}__signals"], z[f"{name}__T"], z[f"{name}__cfg"]
+        cfg = EMDKernelConfig(max_extrema=int(c[0]), nbsym=int(c[1]), max_iteration=int(c[2]),
+                              max_imfs=int(c[3]), real_t=real)
+        L = cfg.build()
+        L._plan.set_variant(4)
+        L._plan.set_tail(1 << 30)
+        imfs, n_imfs, ovf, dn, de, dz = _dense(L, X, T)
+        for b in range(X.shape[0]):
+            assert n_imfs[b] == z[f"{name}__nofma__n_imfs"][b], (name, b)
+            assert ovf[b] == z[f"{name}__nofma__overflow"][b], (name, b)
+            np.testing.assert_array_equal(dn[b], z[f"{name}__nofma__dbg_n"][b])
+            np.testing.assert_array_equal(de[b], z[f"{name}__nofma__dbg_ext"][b])
+            sha = hashlib.sha256(np.ascontiguousarray(imfs[b], dtype=code).tobytes()).hexdigest()
+            assert sha.encode() == z[f"{name}__nofma__sha"][b], (name, b)
+
+
+def test_tail_migration_nbsym_and_small_caps():
+    # other mirror widths and a config that overflows both caps early, with
+    # hand-overs in the middle of IMFs (a batch larger than the threshold)
+    from cuda_emd import EMDKernelConfig, workloads as W
+    X = np.concatenate([W.seismic_batch(600, 1024, seed=12), W.sinusoid_batch(200, 1024, seed=13)])
+    for kw in (dict(nbsym=1), dict(nbsym=3), dict(max_extrema=128, max_iteration=6)):
+        ref = _dense(_moved(EMDKernelConfig(**kw), 0), X)
+        _same(ref, _dense(_moved(EMDKernelConfig(**kw), 300), X))
+
+
+def _moved(cfg, tail):
+    L = cfg.build()
+    L._plan.set_variant(4)
+    L._plan.set_tail(tail)
+    return L
