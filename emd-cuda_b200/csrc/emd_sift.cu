@@ -2395,12 +2395,11 @@ cudaError_t sift_occupancy(int arena_bytes, int variant, int* ctas_per_sm, bool 
 }
 
 cudaError_t launch_sift(const SiftParams& p, int grid, cudaStream_t stream) {
-  // tail migration (p.cont_buf): the 128 x 4 and 256 x 2 builds that hand
-  // over, the 512-thread build that resumes
+  // tail migration (p.cont_buf): the 128 x 4 build that hands over, the
+  // 512-thread build that resumes
   if (p.cont_buf != nullptr) {
     switch (p.variant) {
       case 1: return launch_v<kWideThreads, 1, false, true>(p, grid, stream);
-      case 2: return launch_v<kHalfWideThreads, 2, false, true>(p, grid, stream);
       case 4: return launch_v<kThreads, 4, false, true>(p, grid, stream);
       default: return cudaErrorInvalidValue;
     }

@@ -84,7 +84,7 @@ int emdb_plan_set_variant(emdb_plan* plan, int min_ctas_per_sm);
  * grid is one CTA per signal, kernels.py:1366-1367). */
 int emdb_plan_set_max_ctas(emdb_plan* plan, int max_ctas);
 /* Tail migration for the plan's dense and ragged launches of the 128-thread
- * (4 per SM) and 256-thread instances (no reference counterpart; its launch is one CTA per
+ * instance (4 per SM; no reference counterpart: its launch is one CTA per
  * signal, kernels.py:1366-1367).  Once every trace of a launch has started
  * and at most yield_below of them are still in flight, each stops at its
  * next sift-pass boundary, parks its proto-IMF and loop state in a
