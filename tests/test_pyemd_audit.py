@@ -21,7 +21,8 @@ from oracle import pyemd_default as P
 IMF_RTOL = 1e-9
 
 # Every golden trace whose discrete outputs differ from PyEMD's, with the
-# cause the audit finds (the DESIGN's divergence table lists the same).
+# cause the audit finds (one of the divergence switches of
+# oracle/pyemd_default.py, each a documented difference of the reference).
 EXPECTED = {
     ("tiny6", 0): "ref_zero_count",        # leading exact zero: the parallel scan does not count it
     ("edge512", 0): "ref_zero_count",      # pure tone sin(2 pi 0.05 t): an exact zero at t = 0
